@@ -1,0 +1,371 @@
+#!/usr/bin/env python3
+"""SSSP throughput benchmark (GTEPS) of the B200 persistent consolidation kernel.
+
+Workload (default): R-MAT scale 22 (4,194,304 vertices), edge factor 16
+(67,108,864 generated edges, duplicates and self-loops removed), a=0.57 b=0.19
+c=0.19, uint32 weights uniform in [1,255], seeded synthetic graph (seed 1000),
+source = highest-out-degree vertex.  One step = one full SSSP from that source.
+
+  value    GTEPS = m_r / kernel time (m_r = out-edges of reached vertices), graph
+           resident in HBM, L2 flushed between steps, CUDA events on the launch stream
+  e2e      the same metric through the public host-buffer call nps.sssp(): pinned
+           host CSR -> device, kernel, distances -> host, every step
+  roofline B_alg = 12 m_r + 12 n_r + 4 n bytes per SSSP over the measured HBM peak
+  cpu_baseline  the reference's SSSP_CPU (heap Dijkstra, built from its sources
+           into oracle/_ref) timed on this host, one full SSSP of the workload
+
+`--impl reference` times the reference's CPU SSSP (oracle/_ref, else the oracle
+restatement) on all host cores: the K steps run concurrently, one process each.
+Multi-GPU (torchrun): replicas only -- every rank solves its own copy, the
+value is the sum of edges over the max device time across ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (kind, args, description)
+    "rmat22": ("rmat", dict(scale=22, edge_factor=16, seed=1000),
+               "R-MAT scale 22, edge factor 16, a=.57 b=.19 c=.19, w in [1,255], seed 1000, deduped"),
+    "rmat20": ("rmat", dict(scale=20, edge_factor=16, seed=1),
+               "R-MAT scale 20, edge factor 16, a=.57 b=.19 c=.19, w in [1,255], seed 1, deduped"),
+    "grid4096": ("grid", dict(rows=4096, cols=4096, drop=0.05, wmax=1000, seed=1),
+                 "4096x4096 4-neighbour grid, 5% pairs dropped, w in [1,1000], seed 1, source (0,0)"),
+    "uniform16k": ("uniform", dict(n=16384, m=131072, wmax=100, seed=1),
+                   "uniform random 16,384 vertices / 131,072 edges, w in [1,100], seed 1, source 0"),
+}
+
+# plain autotuned parameters per workload class (overridden by --delta/--level)
+DEFAULT_PARAMS = {
+    "rmat": dict(level=3, threshold=32, block_threshold=256, grid_threshold=4096, delta=64, block_size=256),
+    "grid": dict(level=1, threshold=64, delta=4096, block_size=256),
+    "uniform": dict(level=1, threshold=64, delta=64, block_size=256),
+}
+
+
+def make_graph(nps, name):
+    kind, a, _ = WORKLOADS[name]
+    if kind == "rmat":
+        return nps.gen_rmat(a["scale"], a["edge_factor"], seed=a["seed"])
+    if kind == "grid":
+        return nps.gen_grid(a["rows"], a["cols"], a["drop"], a["wmax"], a["seed"])
+    return nps.gen_uniform(a["n"], a["m"], a["wmax"], a["seed"])
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, copy)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            time.sleep(0.25)
+            self.p.terminate()
+            self.p.wait()
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], None, set()
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's CPU SSSP on all host cores
+
+def _ref_worker(args):
+    path, src, use_ref = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    z = np.load(path)
+    row, col, w = z["row"], z["col"], z["w"]
+    if use_ref:
+        d, t = oracle.ref_sssp_cpu(row, col, w, src)
+    else:
+        d, t = oracle.timed(oracle.sssp_heap, row, col, w, src)
+    return t, oracle.fnv1a(d)
+
+
+def run_reference(a, nps, g, m_r, n_r, cfg):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import multiprocessing as mp
+    import oracle
+    use_ref = oracle.have_reference()
+    cores = os.cpu_count() or 1
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except Exception:
+        avail = 64 << 30
+    per_proc = (g.m * 8 + g.n * 12) * 3 + (m_r * 8) + (110 << 20)
+    procs = max(1, min(a.steps, cores, int(avail * 0.6 // per_proc)))
+    with tempfile.TemporaryDirectory(dir="/dev/shm" if os.path.isdir("/dev/shm") else None) as td:
+        path = os.path.join(td, "g.npz")
+        np.savez(path, row=g.row_ptr, col=g.col, w=g.w)
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(procs) as pool:
+            # warm-up: page in the code and the graph file (one small SSSP per process is not
+            # representative, so warm-up steps are the same call on the same data)
+            t0 = time.perf_counter()
+            res = pool.map(_ref_worker, [(path, g.source, use_ref)] * a.steps)
+            wall = time.perf_counter() - t0
+    times = [r[0] for r in res]
+    value = a.steps * m_r / wall / 1e9
+    line = {
+        "impl": "reference", "metric": "sssp_gteps", "value": value, "unit": "GTEPS", "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * statistics.mean(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic", "config": cfg,
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": procs,
+                         "kind": "reference" if use_ref else "port",
+                         "sample": f"{a.steps} full SSSPs of the workload run concurrently, one process "
+                                   f"each ({procs} at a time), "
+                                   + ("the reference's SSSP_CPU (apps/sssp/src/cpu/sssp.cpp) built from "
+                                      "its sources" if use_ref else "the oracle's restatement of SSSP_CPU")},
+        "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "warmup_note": "CPU code has no warm-up state; the K steps are the timed samples",
+    }
+    return line
+
+
+# ---------------------------------------------------------------------------
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="rmat22", choices=sorted(WORKLOADS))
+    ap.add_argument("--delta", type=int, default=None)
+    ap.add_argument("--level", type=int, default=None)
+    ap.add_argument("--policy", default="plain", choices=["plain", "learned"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    a = ap.parse_args()
+    a.warmup = max(a.warmup, 3)
+
+    ws, rank, local = dist_env()
+    nps = importlib.import_module("nested-parallelism_b200")
+    kind, _, desc = WORKLOADS[a.workload]
+    prm = dict(DEFAULT_PARAMS[kind])
+    if a.delta is not None:
+        prm["delta"] = a.delta
+    if a.level is not None:
+        prm["level"] = a.level
+
+    if a.impl == "reference":
+        if rank != 0:
+            return 0
+        g = make_graph(nps, a.workload)
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        d0 = oracle.sssp_heap(g.row_ptr, g.col, g.w, g.source)
+        n_r, m_r = oracle.reached(g.row_ptr, d0)
+        cfg = {"workload": a.workload, "description": desc, "n": g.n, "m": g.m, "m_reached": m_r,
+               "source": g.source, "parallelism": "host cores"}
+        print(json.dumps(run_reference(a, nps, g, m_r, n_r, cfg)))
+        return 0
+
+    import torch
+    import torch.distributed as dist
+    if ws > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    g = make_graph(nps, a.workload)
+    params = nps.Params(device=local, **prm)
+    if a.policy == "learned":
+        from importlib import import_module
+        pol = import_module("nested-parallelism_b200.policy")
+        wpath = os.path.join(ROOT, "nested-parallelism_b200", "policy_weights.npz")
+        pol.load_into_kernel(pol.MLPWeights.load(wpath), local)
+        params.policy = nps.POLICY_LEARNED
+
+    def to_dev(x):
+        return torch.from_numpy(np.ascontiguousarray(x).view(np.int32)).to(dev)
+
+    row, col, w = to_dev(g.row_ptr), to_dev(g.col), to_dev(g.w)
+    dist_t = torch.empty(g.n, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.int8, device=dev)  # > 126 MB L2
+    stream = torch.cuda.Stream(dev)
+    sptr = stream.cuda_stream
+
+    def step():
+        return nps.sssp_device(row, col, w, g.n, g.m, g.source, dist_t, params, stream=sptr)
+
+    with torch.cuda.stream(stream):
+        for _ in range(a.warmup):
+            st = step()
+    torch.cuda.synchronize(dev)
+    dh = dist_t.cpu().numpy().view(np.uint32)
+    reached = dh < nps.INF
+    n_r = int(reached.sum())
+    m_r = int(np.diff(g.row_ptr)[reached].sum())
+    b_alg = 12 * m_r + 12 * n_r + 4 * g.n
+
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    stats = []
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        wall0 = time.perf_counter()
+        with torch.cuda.stream(stream):
+            for i in range(a.steps):
+                flush.fill_(i & 0x7F)
+                evs[i][0].record(stream)
+                stats.append(step())
+                evs[i][1].record(stream)
+        torch.cuda.synchronize(dev)
+        wall = time.perf_counter() - wall0
+    if ws > 1:
+        dist.barrier()
+    step_ms = [s.elapsed_time(e) for s, e in evs]
+    kern_ms = sum(step_ms)
+    clocks = clk.summary()
+
+    # ---- e2e through the host-buffer public call (pinned host memory)
+    def pinned(x):
+        t = torch.from_numpy(np.ascontiguousarray(x).view(np.int32)).pin_memory()
+        return t.numpy()
+    hg = nps.Graph(pinned(g.row_ptr), pinned(g.col), pinned(g.w).view(np.uint32), g.source)
+    hout = torch.empty(g.n, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+    e2e_steps = a.e2e_steps or a.steps
+    for _ in range(2):
+        nps.sssp(hg, g.source, params, out=hout)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    e2e_dev_ms = []
+    for _ in range(e2e_steps):
+        _, st2 = nps.sssp(hg, g.source, params, out=hout)  # synchronous: H2D + kernel + D2H
+        e2e_dev_ms.append(st2.total_ms)
+    e2e_wall = (time.perf_counter() - t0) / e2e_steps
+    e2e_ok = bool((hout == dh).all())
+
+    tot_t = torch.tensor([kern_ms, e2e_wall * 1e3], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(tot_t, op=dist.ReduceOp.MAX)
+    kern_ms_max, e2e_ms_max = float(tot_t[0]), float(tot_t[1])
+    value = ws * a.steps * m_r / (kern_ms_max * 1e-3) / 1e9
+    e2e_value = ws * m_r / (e2e_ms_max * 1e-3) / 1e9
+
+    peak, peak_src = load_peaks()
+    per_launch_s = kern_ms / a.steps * 1e-3
+    achieved = b_alg / per_launch_s / 1e9
+    traffic = None
+    tr_path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tr_path):
+        with open(tr_path) as f:
+            traffic = json.load(f).get(a.workload)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        if oracle.have_reference():
+            dref, tcpu = oracle.ref_sssp_cpu(g.row_ptr, g.col, g.w, g.source)
+            kind_cpu = "reference"
+            sample = "one full SSSP of the workload by the reference's SSSP_CPU (heap Dijkstra, " \
+                     "apps/sssp/src/cpu/sssp.cpp, built from its sources), 1 thread, including its Heap() init"
+        else:
+            dref, tcpu = oracle.timed(oracle.sssp_heap, g.row_ptr, g.col, g.w, g.source)
+            kind_cpu = "port"
+            sample = "one full SSSP of the workload by the oracle's restated heap Dijkstra, 1 thread"
+        cpu = {"value": m_r / tcpu / 1e9, "unit": "GTEPS", "cores": 1, "kind": kind_cpu, "sample": sample,
+               "seconds": tcpu, "bit_exact_vs_gpu": bool((dref == dh).all())}
+
+    if rank == 0:
+        line = {
+            "metric": "sssp_gteps", "value": value, "unit": "GTEPS", "n_gpus": ws, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": kern_ms_max / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": a.workload, "description": desc, "n": g.n, "m": g.m, "m_reached": m_r,
+                       "n_reached": n_r, "source": g.source, "params": prm, "policy": a.policy,
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
+                       "l2": "flushed between steps (256 MB write); CSR 12 B/edge also exceeds L2",
+                       "iterations": stats[-1].iterations, "buckets": stats[-1].buckets,
+                       "edges_scanned": stats[-1].edges_scanned, "grid_ctas": stats[-1].grid_ctas,
+                       "step_ms_min": min(step_ms), "step_ms_max": max(step_ms), "wall_s": wall},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                         "b_alg_bytes": b_alg, "b_alg_formula": "12*m_r + 12*n_r + 4*n"},
+            "e2e": {"value": e2e_value, "unit": "GTEPS",
+                    "h2d_bytes_per_step": 4 * (g.n + 1) + 8 * g.m, "d2h_bytes_per_step": 4 * g.n,
+                    "ms_per_step": e2e_ms_max, "device_ms_per_step": statistics.mean(e2e_dev_ms),
+                    "bit_exact_vs_device_run": e2e_ok, "call": "nps.sssp(host Graph, pinned)"},
+            "gpu_launches": a.steps,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

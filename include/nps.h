@@ -1,0 +1,238 @@
+/*
+ * nps.h — C ABI of the B200-native single-source shortest path (SSSP) library
+ * with warp / block / grid workload consolidation.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, returns an
+ * `nps_status` (0 = success) and never calls exit().  The message of the last
+ * failure on the calling thread is available from nps_last_error_string().
+ *
+ * Reference interfaces replaced (paths relative to the dadaism/nested-parallelism
+ * source tree):
+ *   nps_sssp / nps_sssp_ctx   replace  void sssp_np_consolidate_gpu(void)
+ *                                       apps/sssp/src/gpu/sssp_wrapper.cu:475-546
+ *                             together with the per-run set-up and tear-down
+ *                             prepare_gpu() / clean_gpu() / SSSP_GPU()
+ *                                       apps/sssp/src/gpu/sssp_wrapper.cu:58-149, :548-583
+ *   nps_sssp_state            replaces the global-state form of the same call: it
+ *                             starts from a caller-supplied cost array and update
+ *                             flags exactly as sssp_np_consolidate_gpu() starts from
+ *                             d_costArray / d_update (sssp_wrapper.cu:22-30, :92-113)
+ *   nps_sssp_batch            has no single counterpart: it runs many independent
+ *                             SSSP_GPU() calls (apps/sssp/src/gpu/sssp.cpp:140-142)
+ *                             in one persistent launch
+ *   nps_read_dimacs9 / _dimacs10 / _slndc
+ *                             replace readInputDIMACS9/10/SLNDC() + convertCSR()
+ *                                       common/global.cpp:29-64, :66-105, :107-190, :192-235
+ *   nps_graph                 replaces struct _GRAPH_'s CSR members and the
+ *                             noNodeTotal / noEdgeTotal / source globals
+ *                                       common/global.h:28-58
+ *
+ * Distances are uint32 with the reference's INF = 2^30 (apps/sssp/src/gpu/
+ * sssp_wrapper.cu:7) for unreachable vertices; a path whose length reaches 2^30
+ * is treated as unreachable, the same sentinel the reference uses.
+ */
+#ifndef NPS_H_
+#define NPS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NPS_INF 0x40000000u  /* 1<<30, apps/sssp/src/gpu/sssp_wrapper.cu:7 */
+#define NPS_ABI_VERSION 1
+
+typedef int32_t nps_status;
+enum {
+  NPS_OK = 0,
+  NPS_ERR_INVALID_ARG = 1,   /* bad size, pointer, source or parameter */
+  NPS_ERR_CUDA = 2,          /* a CUDA runtime call failed */
+  NPS_ERR_CAPACITY = 3,      /* a device queue would have overflowed */
+  NPS_ERR_TIMEOUT = 4,       /* a bounded spin wait in the persistent kernel ran out */
+  NPS_ERR_NO_DEVICE = 5,     /* no CUDA device / wrong architecture */
+  NPS_ERR_IO = 6,            /* file could not be opened or parsed */
+  NPS_ERR_FORMAT = 7,        /* malformed CSR or input file */
+  NPS_ERR_OOM = 8            /* host or device allocation failed */
+};
+
+/* Consolidation granularity for vertices whose out-degree is at least
+ * `threshold` (the reference's THRESHOLD, apps/sssp/src/gpu/sssp_kernel.cu:7).
+ * Values 0..2 are the reference's CONSOLIDATE_LEVEL (sssp_wrapper.cu:503-531). */
+enum {
+  NPS_LEVEL_WARP = 0,   /* per-warp buffer, processed by that warp           (consolidate_warp_dp_kernel,  sssp_kernel.cu:330) */
+  NPS_LEVEL_BLOCK = 1,  /* per-CTA buffer in shared memory, processed by it  (consolidate_block_dp_kernel, sssp_kernel.cu:407) */
+  NPS_LEVEL_GRID = 2,   /* one device-wide buffer, processed by every CTA    (consolidate_grid_dp_kernel,  sssp_kernel.cu:484) */
+  NPS_LEVEL_HYBRID = 3  /* degree ranges [threshold,block_threshold) warp, [block_threshold,grid_threshold) block, rest grid */
+};
+
+enum {
+  NPS_POLICY_PLAIN = 0,    /* fixed delta and level from nps_params */
+  NPS_POLICY_LEARNED = 1   /* per-iteration delta / level from the MLP policy loaded with nps_policy_set_weights */
+};
+
+typedef struct nps_params {
+  int32_t level;            /* NPS_LEVEL_* (default NPS_LEVEL_BLOCK, the reference Makefile's CONSOLIDATE_LEVEL=1) */
+  int32_t threshold;        /* degree at which a vertex is consolidated (default 64) */
+  int32_t block_threshold;  /* NPS_LEVEL_HYBRID only */
+  int32_t grid_threshold;   /* NPS_LEVEL_HYBRID only */
+  int32_t block_size;       /* threads per CTA: 128, 256, 512 or 1024 (default 256) */
+  int32_t ctas_per_sm;      /* resident CTAs per SM; 0 = as many as fit */
+  uint32_t delta;           /* near-far bucket width; 0 = unordered frontier (the reference's order) */
+  int32_t policy;           /* NPS_POLICY_* */
+  int32_t device_ptrs;      /* 1: graph and dist pointers are device pointers; 0: host pointers */
+  int32_t device;           /* CUDA device ordinal */
+  void* stream;             /* cudaStream_t to launch on; NULL = the library's own stream */
+  double timeout_s;         /* bound on every spin wait inside the persistent kernel (default 10 s) */
+  int32_t trace;            /* 1: record one nps_trace_rec per iteration (read with nps_trace_read) */
+  int32_t reserved[7];
+} nps_params;
+
+typedef struct nps_stats {
+  uint32_t iterations;      /* frontier iterations (the reference's `iteration` global) */
+  uint32_t buckets;         /* near-far bucket advances */
+  uint64_t edges_scanned;   /* edge relaxations attempted */
+  uint64_t improvements;    /* successful atomicMin relaxations */
+  uint64_t vertices_processed;
+  uint32_t reached;         /* vertices with a finite distance */
+  uint32_t pad0;
+  uint64_t reached_edges;   /* out-edges of reached vertices (m_r) */
+  float kernel_ms;          /* device time of the persistent launch (CUDA events) */
+  float total_ms;           /* device time including copies done by the call */
+  int32_t status;           /* device status word */
+  int32_t grid_ctas;        /* CTAs in the persistent launch */
+} nps_stats;
+
+/* One record per frontier iteration when nps_params.trace = 1. */
+typedef struct nps_trace_rec {
+  uint32_t iteration;
+  uint32_t frontier;        /* near-queue length processed */
+  uint32_t far_len;         /* far-pile length after the iteration */
+  uint32_t bucket_hi;       /* current bucket upper bound T */
+  uint32_t delta;
+  uint32_t level;
+  uint32_t hist[8];         /* frontier out-degree histogram, bins [4^k-1, 4^(k+1)-1) */
+  uint64_t edges;           /* edges scanned in the iteration */
+  uint64_t improvements;
+  uint32_t reached;         /* vertices reached so far */
+  uint32_t pad;
+} nps_trace_rec;
+
+/* Host-side CSR graph, library-allocated; free with nps_graph_free. */
+typedef struct nps_graph {
+  int32_t n;
+  int32_t source;          /* suggested source: DIMACS9 's' line, 0 otherwise, or the generator's pick */
+  int64_t m;
+  int32_t* row_ptr;        /* n+1 (graph.vertexArray) */
+  int32_t* col;            /* m   (graph.edgeArray)   */
+  uint32_t* w;             /* m   (graph.weightArray) */
+} nps_graph;
+
+typedef struct nps_ctx nps_ctx;
+
+/* ---- library ---------------------------------------------------------- */
+int32_t nps_abi_version(void);
+const char* nps_last_error_string(void);
+void nps_params_default(nps_params* p);
+
+/* ---- graph construction (host) ----------------------------------------- */
+/* Uniform random directed multigraph: each edge draws src and dst uniformly
+ * (self-loops redrawn), weight uniform in [1,wmax]. */
+nps_status nps_gen_uniform(int32_t n, int64_t m, uint32_t wmax, uint64_t seed, nps_graph* out);
+/* R-MAT (no noise), duplicates and self-loops removed; source = highest
+ * out-degree vertex (lowest id on ties). */
+nps_status nps_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c,
+                        uint32_t wmax, uint64_t seed, nps_graph* out);
+/* rows x cols 4-neighbour grid, each undirected pair dropped with probability
+ * drop, independent weights per direction in [1,wmax]; source = vertex 0. */
+nps_status nps_gen_grid(int32_t rows, int32_t cols, double drop, uint32_t wmax, uint64_t seed,
+                        nps_graph* out);
+/* CSR from an edge list in insertion order; rows keep the reverse insertion
+ * order of convertCSR (common/global.cpp:211-225). dedupe=1 keeps the first
+ * of each (src,dst) pair; self-loops are dropped when drop_self_loops=1. */
+nps_status nps_csr_from_edges(int32_t n, int64_t m, const int32_t* src, const int32_t* dst,
+                              const uint32_t* w, int32_t dedupe, int32_t drop_self_loops,
+                              nps_graph* out);
+void nps_graph_free(nps_graph* g);
+/* FNV-1a 64 over n uint32 values (distance-array fingerprint). */
+uint64_t nps_fnv1a_u32(const uint32_t* a, int64_t n);
+
+/* ---- file front-ends: readInput*() + convertCSR() ----------------------- */
+nps_status nps_read_dimacs9(const char* path, nps_graph* out);   /* global.cpp:29-64  */
+nps_status nps_read_dimacs10(const char* path, nps_graph* out);  /* global.cpp:66-105 */
+nps_status nps_read_slndc(const char* path, nps_graph* out);     /* global.cpp:107-190 */
+nps_status nps_write_dimacs9(const char* path, const nps_graph* g, int32_t source);
+
+/* ---- SSSP --------------------------------------------------------------- */
+/* Single source.  row_ptr[n+1], col[m], w[m]; dist_out[n] receives distances
+ * (NPS_INF = unreachable).  Pointers are host or device per p->device_ptrs.
+ * Uses a per-device default context.  p may be NULL (defaults). */
+nps_status nps_sssp(const int32_t* row_ptr, const int32_t* col, const uint32_t* w, int32_t n,
+                    int64_t m, int32_t src, const nps_params* p, uint32_t* dist_out,
+                    nps_stats* st);
+
+/* Same, through an explicit context (its own stream and cached workspace). */
+nps_status nps_ctx_create(int32_t device, nps_ctx** out);
+nps_status nps_ctx_destroy(nps_ctx* ctx);
+nps_status nps_sssp_ctx(nps_ctx* ctx, const int32_t* row_ptr, const int32_t* col,
+                        const uint32_t* w, int32_t n, int64_t m, int32_t src,
+                        const nps_params* p, uint32_t* dist_out, nps_stats* st);
+
+/* Start from an existing state, as sssp_np_consolidate_gpu() does: cost[n] holds
+ * the initial distances and is updated in place; every vertex with update[v] != 0
+ * is in the initial frontier; update[] is cleared on return.  Device pointers only. */
+nps_status nps_sssp_state(const int32_t* d_row_ptr, const int32_t* d_col, const uint32_t* d_w,
+                          int32_t n, int64_t m, uint32_t* d_cost, uint8_t* d_update,
+                          const nps_params* p, nps_stats* st);
+
+/* Copy the per-iteration trace of the last traced call on this thread's default
+ * context for `device` (at most cap records); returns the record count in *count. */
+nps_status nps_trace_read(int32_t device, nps_trace_rec* out, int32_t cap, int32_t* count);
+
+/* ---- batched SSSP -------------------------------------------------------- */
+typedef struct nps_instance {
+  const int32_t* row_ptr;  /* device pointers */
+  const int32_t* col;
+  const uint32_t* w;
+  uint32_t* dist;          /* device, n entries */
+  int32_t n;
+  int32_t src;
+  int64_t m;
+} nps_instance;
+
+/* Run `count` independent instances in one persistent cooperative launch; CTAs
+ * are split into teams (one team per group of instances, sized by edge count).
+ * With use_graph = 1 the launch is captured into a CUDA graph on the first call
+ * for this instance set and replayed on later calls with the same set. */
+nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, const nps_params* p,
+                          int32_t use_graph, nps_stats* per_instance, float* kernel_ms);
+
+/* ---- learned policy (MLP 12 -> 32 -> 14) --------------------------------- */
+#define NPS_MLP_IN 12
+#define NPS_MLP_HID 32
+#define NPS_MLP_OUT 14   /* 11 delta logits (2^0..2^10) + 3 level logits */
+/* Load policy weights (fp32 in; stored on the device as bf16): W1[32x12], b1[32],
+ * W2[14x32], b2[14], plus the 12 feature means and 12 inverse std devs. */
+nps_status nps_policy_set_weights(int32_t device, const float* w1, const float* b1,
+                                  const float* w2, const float* b2, const float* feat_mean,
+                                  const float* feat_istd);
+/* MLP training step kernels (device pointers, bf16 weights held as uint16 bits,
+ * fp32 master copies and gradients). X[B x 12] fp32 features (already normalised),
+ * label_delta[B] in 0..10, label_level[B] in 0..2, sample weight wt[B]. */
+nps_status nps_mlp_forward(const uint16_t* w1, const float* b1, const uint16_t* w2,
+                           const float* b2, const float* X, int32_t B, float* logits,
+                           void* stream);
+nps_status nps_mlp_loss_backward(const uint16_t* w1, const float* b1, const uint16_t* w2,
+                                 const float* b2, const float* X, const int32_t* label_delta,
+                                 const int32_t* label_level, const float* wt, int32_t B,
+                                 float* g_w1, float* g_b1, float* g_w2, float* g_b2,
+                                 float* loss, void* stream);
+nps_status nps_mlp_adam_step(float* master, uint16_t* bf16_out, const float* grad, float* m1,
+                             float* m2, int32_t count, float lr, float beta1, float beta2,
+                             float eps, int32_t step, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NPS_H_ */

@@ -1,0 +1,346 @@
+"""B200-native single-source shortest paths with warp / block / grid workload
+consolidation -- the Python face of libnps.so.
+
+The names mirror the reference's SSSP path (dadaism/nested-parallelism):
+
+  readInputDIMACS9 / readInputDIMACS10 / readInputSLNDC   common/global.cpp:29-190
+  convertCSR                                              common/global.cpp:192-235
+  SSSP_GPU                                                apps/sssp/src/gpu/sssp_wrapper.cu:548-583
+  sssp_np_consolidate_gpu                                 apps/sssp/src/gpu/sssp_wrapper.cu:475-546
+  CONSOLIDATE_WARP/BLOCK/GRID (CONSOLIDATE_LEVEL 0/1/2)   apps/sssp/src/gpu/sssp_wrapper.cu:503-531
+  THRESHOLD = 64                                          apps/sssp/src/gpu/sssp_kernel.cu:7
+  INF = 2^30                                              apps/sssp/src/gpu/sssp_wrapper.cu:7
+
+Where the reference calls exit() on an error this module raises NpsError.
+Every compute call runs the CUDA kernels of libnps.so; there is no CPU path.
+Import it as importlib.import_module("nested-parallelism_b200").
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Iterable, List, Optional, Sequence
+
+import numpy as np
+
+from ._native import (NPS_INF, NPS_MLP_HID, NPS_MLP_IN, NPS_MLP_OUT, NpsError, check, lib,
+                      nps_graph, nps_instance, nps_params, nps_stats, nps_trace_rec)
+
+INF = NPS_INF
+THRESHOLD = 64
+CONSOLIDATE_WARP, CONSOLIDATE_BLOCK, CONSOLIDATE_GRID, CONSOLIDATE_HYBRID = 0, 1, 2, 3
+POLICY_PLAIN, POLICY_LEARNED = 0, 1
+SOLUTION_CONSOLIDATE = 6  # `-s 6`, apps/sssp/src/gpu/sssp.cpp:38
+
+__all__ = [
+    "INF", "THRESHOLD", "CONSOLIDATE_WARP", "CONSOLIDATE_BLOCK", "CONSOLIDATE_GRID",
+    "CONSOLIDATE_HYBRID", "POLICY_PLAIN", "POLICY_LEARNED", "Graph", "Params", "Stats",
+    "NpsError", "gen_uniform", "gen_rmat", "gen_grid", "convertCSR", "readInputDIMACS9",
+    "readInputDIMACS10", "readInputSLNDC", "writeDIMACS9", "sssp", "sssp_device", "SSSP_GPU",
+    "sssp_np_consolidate_gpu", "sssp_batch", "trace_read", "fnv1a", "abi_version", "lib",
+]
+
+
+def abi_version() -> int:
+    return int(lib.nps_abi_version())
+
+
+# ---------------------------------------------------------------------------
+# graphs
+
+@dataclass
+class Graph:
+    """CSR graph: the struct _GRAPH_ members and noNodeTotal / noEdgeTotal /
+    source globals of common/global.h:28-58."""
+    vertexArray: np.ndarray  # int32 [n+1]
+    edgeArray: np.ndarray    # int32 [m]
+    weightArray: np.ndarray  # uint32 [m]
+    source: int = 0
+
+    @property
+    def noNodeTotal(self) -> int:
+        return int(self.vertexArray.shape[0] - 1)
+
+    @property
+    def noEdgeTotal(self) -> int:
+        return int(self.edgeArray.shape[0])
+
+    n = noNodeTotal
+    m = noEdgeTotal
+
+    @property
+    def row_ptr(self) -> np.ndarray:
+        return self.vertexArray
+
+    @property
+    def col(self) -> np.ndarray:
+        return self.edgeArray
+
+    @property
+    def w(self) -> np.ndarray:
+        return self.weightArray
+
+    def degrees(self) -> np.ndarray:
+        return np.diff(self.vertexArray)
+
+
+def _take(g: nps_graph) -> Graph:
+    try:
+        n, m = int(g.n), int(g.m)
+        row = np.ctypeslib.as_array(g.row_ptr, shape=(n + 1,)).copy()
+        col = np.ctypeslib.as_array(g.col, shape=(max(m, 1),))[:m].copy()
+        w = np.ctypeslib.as_array(g.w, shape=(max(m, 1),))[:m].copy()
+        return Graph(row, col, w, int(g.source))
+    finally:
+        lib.nps_graph_free(C.byref(g))
+
+
+def gen_uniform(n: int, m: int, wmax: int = 100, seed: int = 1) -> Graph:
+    """Uniform random directed graph: each edge picks src and dst uniformly
+    (self-loops redrawn), weight uniform in [1, wmax]; source 0."""
+    g = nps_graph()
+    check(lib.nps_gen_uniform(n, m, wmax, seed, C.byref(g)), "gen_uniform")
+    return _take(g)
+
+
+def gen_rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+             wmax: int = 255, seed: int = 1) -> Graph:
+    """R-MAT graph (no noise), duplicates and self-loops removed; source is the
+    highest-out-degree vertex (lowest id on ties)."""
+    g = nps_graph()
+    check(lib.nps_gen_rmat(scale, edge_factor, a, b, c, wmax, seed, C.byref(g)), "gen_rmat")
+    return _take(g)
+
+
+def gen_grid(rows: int, cols: int, drop: float = 0.05, wmax: int = 1000, seed: int = 1) -> Graph:
+    """4-neighbour grid, each undirected pair dropped with probability `drop`,
+    independent weights per direction in [1, wmax]; source (0, 0)."""
+    g = nps_graph()
+    check(lib.nps_gen_grid(rows, cols, drop, wmax, seed, C.byref(g)), "gen_grid")
+    return _take(g)
+
+
+def convertCSR(n: int, src, dst, w, dedupe: bool = False, drop_self_loops: bool = False) -> Graph:
+    """Edge list (in insertion order) to CSR with every row in reverse insertion
+    order, as convertCSR() lays out the adjacency lists (global.cpp:211-225)."""
+    s = np.ascontiguousarray(src, dtype=np.int32)
+    d = np.ascontiguousarray(dst, dtype=np.int32)
+    ww = np.ascontiguousarray(w, dtype=np.uint32)
+    if not (s.shape == d.shape == ww.shape):
+        raise ValueError("src, dst and w must have the same length")
+    g = nps_graph()
+    check(lib.nps_csr_from_edges(n, s.shape[0], s.ctypes.data, d.ctypes.data, ww.ctypes.data,
+                                 int(dedupe), int(drop_self_loops), C.byref(g)), "convertCSR")
+    return _take(g)
+
+
+def _read(fn, path: str, where: str) -> Graph:
+    g = nps_graph()
+    check(fn(str(path).encode(), C.byref(g)), where)
+    return _take(g)
+
+
+def readInputDIMACS9(path: str) -> Graph:
+    return _read(lib.nps_read_dimacs9, path, "readInputDIMACS9")
+
+
+def readInputDIMACS10(path: str) -> Graph:
+    return _read(lib.nps_read_dimacs10, path, "readInputDIMACS10")
+
+
+def readInputSLNDC(path: str) -> Graph:
+    return _read(lib.nps_read_slndc, path, "readInputSLNDC")
+
+
+def _as_nps_graph(g: Graph) -> nps_graph:
+    row = np.ascontiguousarray(g.vertexArray, dtype=np.int32)
+    col = np.ascontiguousarray(g.edgeArray, dtype=np.int32)
+    w = np.ascontiguousarray(g.weightArray, dtype=np.uint32)
+    ng = nps_graph()
+    ng.n, ng.m, ng.source = row.shape[0] - 1, col.shape[0], int(g.source)
+    ng.row_ptr = row.ctypes.data_as(C.POINTER(C.c_int32))
+    ng.col = col.ctypes.data_as(C.POINTER(C.c_int32))
+    ng.w = w.ctypes.data_as(C.POINTER(C.c_uint32))
+    ng._keep = (row, col, w)  # keep the buffers alive with the struct
+    return ng
+
+
+def writeDIMACS9(path: str, g: Graph, source: Optional[int] = None) -> None:
+    ng = _as_nps_graph(g)
+    check(lib.nps_write_dimacs9(str(path).encode(), C.byref(ng), g.source if source is None else source),
+          "writeDIMACS9")
+
+
+def fnv1a(dist: np.ndarray) -> int:
+    a = np.ascontiguousarray(dist, dtype=np.uint32)
+    return int(lib.nps_fnv1a_u32(a.ctypes.data, a.shape[0]))
+
+
+# ---------------------------------------------------------------------------
+# parameters and statistics
+
+@dataclass
+class Params:
+    level: int = CONSOLIDATE_BLOCK      # CONSOLIDATE_LEVEL (Makefile default 1)
+    threshold: int = THRESHOLD
+    block_threshold: int = 256
+    grid_threshold: int = 4096
+    block_size: int = 256
+    ctas_per_sm: int = 0
+    delta: int = 0                      # 0 = the reference's unordered frontier
+    policy: int = POLICY_PLAIN
+    device: int = 0
+    timeout_s: float = 10.0
+    trace: bool = False
+    fault_inject_wait: bool = False     # test hook: the first barrier can never complete
+
+    def to_c(self, device_ptrs: bool, stream: Optional[int] = None) -> nps_params:
+        p = nps_params()
+        lib.nps_params_default(C.byref(p))
+        p.level, p.threshold = self.level, self.threshold
+        p.block_threshold, p.grid_threshold = self.block_threshold, self.grid_threshold
+        p.block_size, p.ctas_per_sm, p.delta = self.block_size, self.ctas_per_sm, self.delta
+        p.policy, p.device, p.timeout_s = self.policy, self.device, float(self.timeout_s)
+        p.trace = int(bool(self.trace))
+        p.device_ptrs = int(bool(device_ptrs))
+        p.stream = stream
+        p.reserved[0] = int(bool(self.fault_inject_wait))
+        return p
+
+
+@dataclass
+class Stats:
+    iterations: int = 0
+    buckets: int = 0
+    edges_scanned: int = 0
+    improvements: int = 0
+    vertices_processed: int = 0
+    reached: int = 0
+    kernel_ms: float = 0.0
+    total_ms: float = 0.0
+    status: int = 0
+    grid_ctas: int = 0
+
+    @staticmethod
+    def from_c(s: nps_stats) -> "Stats":
+        return Stats(int(s.iterations), int(s.buckets), int(s.edges_scanned), int(s.improvements),
+                     int(s.vertices_processed), int(s.reached), float(s.kernel_ms), float(s.total_ms),
+                     int(s.status), int(s.grid_ctas))
+
+
+def _ptr(x) -> int:
+    """Device pointer of a tensor-like object (data_ptr()) or a raw int."""
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return int(x.data_ptr())
+    raise TypeError(f"expected a device pointer or an object with data_ptr(), got {type(x)!r}")
+
+
+# ---------------------------------------------------------------------------
+# SSSP
+
+def sssp(g: Graph, source: Optional[int] = None, params: Optional[Params] = None,
+         out: Optional[np.ndarray] = None):
+    """Shortest distances from `source` on host CSR arrays.  The call copies the
+    graph to the device, runs one persistent launch and copies distances back.
+    Returns (dist uint32[n], Stats); unreachable vertices hold INF."""
+    p = params or Params()
+    src = g.source if source is None else int(source)
+    row = np.ascontiguousarray(g.vertexArray, dtype=np.int32)
+    col = np.ascontiguousarray(g.edgeArray, dtype=np.int32)
+    w = np.ascontiguousarray(g.weightArray, dtype=np.uint32)
+    n = row.shape[0] - 1
+    dist = out if out is not None else np.empty(n, dtype=np.uint32)
+    if dist.dtype != np.uint32 or dist.shape[0] != n or not dist.flags.c_contiguous:
+        raise ValueError("out must be a contiguous uint32 array of n entries")
+    st = nps_stats()
+    cp = p.to_c(device_ptrs=False)
+    check(lib.nps_sssp(row.ctypes.data, col.ctypes.data, w.ctypes.data, n, col.shape[0], src,
+                       C.byref(cp), dist.ctypes.data, C.byref(st)), "sssp")
+    return dist, Stats.from_c(st)
+
+
+def sssp_device(row_ptr, col, w, n: int, m: int, src: int, dist_out,
+                params: Optional[Params] = None, stream: Optional[int] = None) -> Stats:
+    """Same on device-resident arrays (tensors or raw pointers); launches on
+    `stream` (a cudaStream_t as int) when given, else on the library's stream."""
+    p = params or Params()
+    st = nps_stats()
+    cp = p.to_c(device_ptrs=True, stream=stream)
+    check(lib.nps_sssp(_ptr(row_ptr), _ptr(col), _ptr(w), n, m, src, C.byref(cp), _ptr(dist_out),
+                       C.byref(st)), "sssp_device")
+    return Stats.from_c(st)
+
+
+def SSSP_GPU(g: Graph, solution: int = SOLUTION_CONSOLIDATE, level: int = CONSOLIDATE_BLOCK,
+             params: Optional[Params] = None) -> np.ndarray:
+    """graph.costArray after one SSSP_GPU() run (sssp_wrapper.cu:548-583): int32
+    costs with INF = 2^30 for unreachable vertices.  Only solution 6 (workload
+    consolidation) is provided by this library."""
+    if solution != SOLUTION_CONSOLIDATE:
+        raise NpsError(1, f"SSSP_GPU: solution {solution} is not provided (only 6, workload consolidation)")
+    p = params or Params(level=level)
+    dist, _ = sssp(g, g.source, p)
+    return dist.view(np.int32)
+
+
+def sssp_np_consolidate_gpu(d_vertexArray, d_edgeArray, d_weightArray, d_costArray, d_update,
+                            noNodeTotal: int, noEdgeTotal: int, level: int = CONSOLIDATE_BLOCK,
+                            params: Optional[Params] = None, stream: Optional[int] = None) -> Stats:
+    """The state form of sssp_np_consolidate_gpu() (sssp_wrapper.cu:475-546):
+    device arrays as prepare_gpu() leaves them -- d_costArray int32 (INF except
+    the source), d_update uint8 flags (the source set).  Costs are updated in
+    place and d_update is cleared.  Returns Stats (Stats.iterations is the
+    reference's `iteration` counter)."""
+    p = params or Params(level=level)
+    st = nps_stats()
+    cp = p.to_c(device_ptrs=True, stream=stream)
+    check(lib.nps_sssp_state(_ptr(d_vertexArray), _ptr(d_edgeArray), _ptr(d_weightArray), noNodeTotal,
+                             noEdgeTotal, _ptr(d_costArray), _ptr(d_update), C.byref(cp), C.byref(st)),
+          "sssp_np_consolidate_gpu")
+    return Stats.from_c(st)
+
+
+@dataclass
+class Instance:
+    """One batched SSSP instance on device-resident arrays."""
+    row_ptr: object
+    col: object
+    w: object
+    dist: object
+    n: int
+    m: int
+    src: int
+
+
+def sssp_batch(instances: Sequence[Instance], params: Optional[Params] = None, use_graph: bool = True,
+               stream: Optional[int] = None):
+    """Run many independent instances in one persistent cooperative launch
+    (captured into a CUDA graph and replayed when use_graph).  Returns
+    (list[Stats], kernel_ms)."""
+    p = params or Params()
+    k = len(instances)
+    arr = (nps_instance * k)()
+    for i, x in enumerate(instances):
+        arr[i].row_ptr, arr[i].col, arr[i].w, arr[i].dist = _ptr(x.row_ptr), _ptr(x.col), _ptr(x.w), _ptr(x.dist)
+        arr[i].n, arr[i].m, arr[i].src = int(x.n), int(x.m), int(x.src)
+    stats = (nps_stats * k)()
+    ms = C.c_float(0.0)
+    cp = p.to_c(device_ptrs=True, stream=stream)
+    check(lib.nps_sssp_batch(arr, k, C.byref(cp), int(bool(use_graph)), stats, C.byref(ms)), "sssp_batch")
+    return [Stats.from_c(s) for s in stats], float(ms.value)
+
+
+def trace_read(device: int = 0, cap: int = 1 << 16) -> List[dict]:
+    """Per-iteration records of the last call made with Params(trace=True)."""
+    buf = (nps_trace_rec * cap)()
+    cnt = C.c_int32(0)
+    check(lib.nps_trace_read(device, buf, cap, C.byref(cnt)), "trace_read")
+    out = []
+    for r in buf[: cnt.value]:
+        out.append(dict(iteration=r.iteration, frontier=r.frontier, far_len=r.far_len,
+                        bucket_hi=r.bucket_hi, delta=r.delta, level=r.level, hist=list(r.hist),
+                        edges=int(r.edges), improvements=int(r.improvements), reached=r.reached,
+                        heavy=r.pad))
+    return out

@@ -1,0 +1,858 @@
+// Host engine of the SSSP library: contexts, workspaces, the cooperative
+// launch of the persistent kernel and the C ABI of include/nps.h.
+//
+// Boundary.  nps_sssp()/nps_sssp_ctx() take the place of the reference's
+// SSSP_GPU() + sssp_np_consolidate_gpu() pair (apps/sssp/src/gpu/
+// sssp_wrapper.cu:548-583, :475-546): where the reference resets the device,
+// allocates five arrays and two queues, and loops on the host until the queue
+// is empty, a call here reuses a cached per-context workspace and makes exactly
+// one persistent launch.  Errors come back as status codes instead of exit().
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "nps.h"
+#include "nps_device.cuh"
+#include "nps_internal.h"
+
+using nps::Counters;
+using nps::InstDesc;
+using nps::LaunchParams;
+using nps::PolicyDev;
+using nps::TeamDesc;
+
+// ---------------------------------------------------------------------------
+// errors
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+nps_status nps_fail(nps_status code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+void nps_clear_error() { g_last_error.clear(); }
+
+extern "C" const char* nps_last_error_string(void) { return g_last_error.c_str(); }
+extern "C" int32_t nps_abi_version(void) { return NPS_ABI_VERSION; }
+
+#define NPS_CUDA(call)                                                                       \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return nps_fail(NPS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+
+extern "C" void nps_params_default(nps_params* p) {
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  p->level = NPS_LEVEL_BLOCK;
+  p->threshold = 64;
+  p->block_threshold = 256;
+  p->grid_threshold = 4096;
+  p->block_size = 256;
+  p->ctas_per_sm = 0;
+  p->delta = 0;
+  p->policy = NPS_POLICY_PLAIN;
+  p->device_ptrs = 0;
+  p->device = 0;
+  p->stream = nullptr;
+  p->timeout_s = 10.0;
+  p->trace = 0;
+}
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// device properties
+
+struct DevInfo {
+  bool ok = false;
+  int sms = 0;
+  int major = 0, minor = 0;
+  bool coop = false;
+};
+
+nps_status device_info(int dev, DevInfo* out) {
+  static std::mutex mu;
+  static std::vector<DevInfo> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return nps_fail(NPS_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  }
+  if (dev < 0 || dev >= count) return nps_fail(NPS_ERR_INVALID_ARG, "device ordinal out of range");
+  if ((int)cache.size() < count) cache.resize(count);
+  if (!cache[dev].ok) {
+    cudaDeviceProp pr;
+    NPS_CUDA(cudaGetDeviceProperties(&pr, dev));
+    int coop = 0;
+    NPS_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    cache[dev].sms = pr.multiProcessorCount;
+    cache[dev].major = pr.major;
+    cache[dev].minor = pr.minor;
+    cache[dev].coop = coop != 0;
+    cache[dev].ok = true;
+  }
+  *out = cache[dev];
+  if (out->major != 10)
+    return nps_fail(NPS_ERR_NO_DEVICE, "libnps is built for sm_100a (B200); device has compute capability " +
+                                           std::to_string(out->major) + "." + std::to_string(out->minor));
+  if (!out->coop) return nps_fail(NPS_ERR_NO_DEVICE, "device does not support cooperative launch");
+  return NPS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// kernel selection
+
+using KernelFn = void (*)(const LaunchParams, const InstDesc);
+
+KernelFn pick_kernel(int bs, bool single) {
+  switch (bs) {
+    case 128: return single ? nps::sssp_persistent_kernel<128, true> : nps::sssp_persistent_kernel<128, false>;
+    case 256: return single ? nps::sssp_persistent_kernel<256, true> : nps::sssp_persistent_kernel<256, false>;
+    case 512: return single ? nps::sssp_persistent_kernel<512, true> : nps::sssp_persistent_kernel<512, false>;
+    default: return nullptr;
+  }
+}
+
+nps_status grid_size(int dev, const DevInfo& di, int bs, bool single, int ctas_per_sm, int* grid) {
+  KernelFn k = pick_kernel(bs, single);
+  if (!k) return nps_fail(NPS_ERR_INVALID_ARG, "block_size must be 128, 256 or 512");
+  int nb = 0;
+  NPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)k, bs, 0));
+  if (nb <= 0) return nps_fail(NPS_ERR_CUDA, "persistent kernel does not fit on an SM");
+  if (ctas_per_sm > 0) nb = std::min(nb, ctas_per_sm);
+  *grid = nb * di.sms;
+  (void)dev;
+  return NPS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// device buffers
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  nps_status ensure(size_t count, bool zero, cudaStream_t s) {
+    if (count <= n && p) return NPS_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+      return nps_fail(NPS_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    n = count;
+    if (zero) {
+      e = cudaMemsetAsync(p, 0, std::max<size_t>(count, 1) * sizeof(T), s);
+      if (e != cudaSuccess) return nps_fail(NPS_ERR_CUDA, cudaGetErrorString(e));
+    }
+    return NPS_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+// Control block: counters, barrier words and the abort flag share one
+// allocation so a single memset clears them before each launch.
+struct Control {
+  size_t n_inst = 0, n_teams = 0;
+  char* base = nullptr;
+  size_t bytes = 0;
+  Counters* ctr() const { return (Counters*)base; }
+  uint32_t* bar() const { return (uint32_t*)(base + n_inst * sizeof(Counters)); }
+  uint32_t* abort_flag() const { return bar() + 32 * n_teams; }
+};
+
+struct PolicyState {
+  PolicyDev* dev = nullptr;
+  bool set = false;
+};
+
+std::mutex g_policy_mu;
+std::vector<PolicyState> g_policy;
+
+}  // namespace
+
+struct nps_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  DevInfo di;
+  // per-instance workspace (single-instance calls)
+  DevBuf<int32_t> q0, q1, f0, f1;
+  DevBuf<uint32_t> mark, fmark, stamp;
+  DevBuf<int4> heavy;
+  DevBuf<char> control;
+  DevBuf<nps_trace_rec> trace;
+  uint32_t trace_count = 0;
+  // graph staging for host-pointer calls
+  DevBuf<int32_t> g_row, g_col;
+  DevBuf<uint32_t> g_w, g_dist;
+  // batch workspace
+  DevBuf<int32_t> b_pool;
+  DevBuf<uint32_t> b_stamp;
+  DevBuf<int4> b_heavy;
+  DevBuf<InstDesc> b_inst;
+  DevBuf<TeamDesc> b_teams;
+  DevBuf<int32_t> b_order;
+  DevBuf<char> b_control;
+  std::vector<InstDesc> b_inst_host;
+  std::vector<nps_instance> b_key;
+  nps_params b_params_key{};
+  int b_grid = 0, b_bs = 0;
+  int b_nteams = 0;
+  cudaGraphExec_t b_graph = nullptr;
+  Counters* h_ctr = nullptr;  // pinned
+  size_t h_ctr_n = 0;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  std::mutex mu;
+};
+
+namespace {
+
+nps_status ctx_init(nps_ctx* c, int device) {
+  nps_status st = device_info(device, &c->di);
+  if (st != NPS_OK) return st;
+  c->device = device;
+  NPS_CUDA(cudaSetDevice(device));
+  NPS_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  for (auto& e : c->ev) NPS_CUDA(cudaEventCreate(&e));
+  return NPS_OK;
+}
+
+void ctx_release(nps_ctx* c) {
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto* b : {&c->q0, &c->q1, &c->f0, &c->f1, &c->g_row, &c->g_col, &c->b_pool, &c->b_order}) b->release();
+  for (auto* b : {&c->mark, &c->fmark, &c->stamp, &c->g_w, &c->g_dist, &c->b_stamp}) b->release();
+  c->heavy.release();
+  c->b_heavy.release();
+  c->control.release();
+  c->b_control.release();
+  c->trace.release();
+  c->b_inst.release();
+  c->b_teams.release();
+  if (c->b_graph) cudaGraphExecDestroy(c->b_graph);
+  c->b_graph = nullptr;
+  if (c->h_ctr) cudaFreeHost(c->h_ctr);
+  c->h_ctr = nullptr;
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  c->stream = nullptr;
+}
+
+nps_status ensure_pinned_counters(nps_ctx* c, size_t n) {
+  if (c->h_ctr_n >= n && c->h_ctr) return NPS_OK;
+  if (c->h_ctr) cudaFreeHost(c->h_ctr);
+  c->h_ctr = nullptr;
+  c->h_ctr_n = 0;
+  NPS_CUDA(cudaMallocHost(&c->h_ctr, n * sizeof(Counters)));
+  c->h_ctr_n = n;
+  return NPS_OK;
+}
+
+// Default context per device (created on first use, lives until exit).
+std::mutex g_ctx_mu;
+std::vector<nps_ctx*> g_default_ctx;
+
+nps_status default_ctx(int device, nps_ctx** out) {
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (device < 0) return nps_fail(NPS_ERR_INVALID_ARG, "device ordinal out of range");
+  if ((int)g_default_ctx.size() <= device) g_default_ctx.resize(device + 1, nullptr);
+  if (!g_default_ctx[device]) {
+    auto* c = new nps_ctx();
+    nps_status st = ctx_init(c, device);
+    if (st != NPS_OK) {
+      delete c;
+      return st;
+    }
+    g_default_ctx[device] = c;
+  }
+  *out = g_default_ctx[device];
+  return NPS_OK;
+}
+
+nps_status check_params(const nps_params& p) {
+  if (p.level < 0 || p.level > 3) return nps_fail(NPS_ERR_INVALID_ARG, "level must be 0..3");
+  if (p.threshold < 1) return nps_fail(NPS_ERR_INVALID_ARG, "threshold must be >= 1");
+  if (p.level == NPS_LEVEL_HYBRID && (p.block_threshold < p.threshold || p.grid_threshold < p.block_threshold))
+    return nps_fail(NPS_ERR_INVALID_ARG, "hybrid thresholds must satisfy threshold <= block_threshold <= grid_threshold");
+  if (p.block_size != 128 && p.block_size != 256 && p.block_size != 512)
+    return nps_fail(NPS_ERR_INVALID_ARG, "block_size must be 128, 256 or 512");
+  if (p.ctas_per_sm < 0) return nps_fail(NPS_ERR_INVALID_ARG, "ctas_per_sm must be >= 0");
+  if (p.policy != NPS_POLICY_PLAIN && p.policy != NPS_POLICY_LEARNED)
+    return nps_fail(NPS_ERR_INVALID_ARG, "policy must be 0 (plain) or 1 (learned)");
+  if (!(p.timeout_s > 0) || p.timeout_s > 3600) return nps_fail(NPS_ERR_INVALID_ARG, "timeout_s must be in (0, 3600]");
+  if (p.delta >= NPS_INF) return nps_fail(NPS_ERR_INVALID_ARG, "delta must be < 2^30");
+  return NPS_OK;
+}
+
+// Smallest degree that can reach the grid tier under these parameters
+// (bounds the number of grid-tier entries per iteration by m / t + 1).
+int32_t min_grid_threshold(const nps_params& p) {
+  int32_t t = p.level == NPS_LEVEL_HYBRID ? p.grid_threshold : p.threshold;
+  if (p.policy == NPS_POLICY_LEARNED) t = std::min(t, p.threshold);
+  return std::max(t, 1);
+}
+
+uint32_t heavy_capacity(int32_t n, int64_t m, const nps_params& p) {
+  // two halves (iteration parity), each bounded by the vertex count and m / t
+  int64_t per = std::min<int64_t>((int64_t)n, m / min_grid_threshold(p) + 1);
+  return (uint32_t)std::max<int64_t>(2 * per, 2);
+}
+
+PolicyDev* policy_ptr(int device) {
+  std::lock_guard<std::mutex> lk(g_policy_mu);
+  if ((int)g_policy.size() <= device || !g_policy[device].set) return nullptr;
+  return g_policy[device].dev;
+}
+
+void fill_thresholds(const nps_params& p, InstDesc& d) {
+  d.level = p.level;
+  d.t1 = p.threshold;
+  d.t2 = p.block_threshold;
+  d.t3 = p.grid_threshold;
+  d.delta = p.delta;
+  d.policy = p.policy;
+}
+
+// Whole-launch bound: 30 per-wait timeouts, at least 60 s.
+unsigned long long run_budget_ns(const nps_params& p) {
+  return (unsigned long long)(std::max(60.0, 30.0 * p.timeout_s) * 1e9);
+}
+
+nps_status launch(nps_ctx* c, cudaStream_t s, int bs, bool single, int grid, const LaunchParams& lp,
+                  const InstDesc& inst) {
+  KernelFn k = pick_kernel(bs, single);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)bs);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  (void)c;
+  NPS_CUDA(cudaLaunchKernelEx(&cfg, k, lp, inst));
+  return NPS_OK;
+}
+
+nps_status status_from_device(uint32_t st) {
+  switch (st) {
+    case NPS_OK: return NPS_OK;
+    case NPS_ERR_CAPACITY: return nps_fail(NPS_ERR_CAPACITY, "device queue capacity exceeded");
+    case NPS_ERR_TIMEOUT: return nps_fail(NPS_ERR_TIMEOUT, "a bounded wait in the persistent kernel timed out");
+    case NPS_ERR_FORMAT: return nps_fail(NPS_ERR_FORMAT, "malformed CSR: a row range or neighbour id is out of bounds");
+    default: return nps_fail((nps_status)st, "device reported error " + std::to_string(st));
+  }
+}
+
+// Core single-instance run on device-resident arrays.
+nps_status run_single(nps_ctx* c, cudaStream_t s, const int32_t* row, const int32_t* col, const uint32_t* w,
+                      int32_t n, int64_t m, int32_t src, uint32_t* dist, uint8_t* update, int mode,
+                      const nps_params& p, nps_stats* st, bool time_it) {
+  const size_t nn = (size_t)n;
+  nps_status e;
+  if ((e = c->q0.ensure(nn, false, s)) || (e = c->q1.ensure(nn, false, s)) || (e = c->f0.ensure(nn, false, s)) ||
+      (e = c->f1.ensure(nn, false, s)))
+    return e;
+  const bool grow_marks = c->mark.n < nn;
+  if ((e = c->mark.ensure(nn, true, s)) || (e = c->fmark.ensure(nn, true, s))) return e;
+  if ((e = c->stamp.ensure(1, grow_marks || !c->stamp.p, s))) return e;
+  if (grow_marks) NPS_CUDA(cudaMemsetAsync(c->stamp.p, 0, sizeof(uint32_t), s));
+  const uint32_t hcap = heavy_capacity(n, m, p);
+  if ((e = c->heavy.ensure(hcap, false, s))) return e;
+  Control ctl;
+  ctl.n_inst = 1;
+  ctl.n_teams = 1;
+  ctl.bytes = sizeof(Counters) + 32 * sizeof(uint32_t) + 128;
+  if ((e = c->control.ensure(ctl.bytes, false, s))) return e;
+  ctl.base = c->control.p;
+  if (p.trace) {
+    if ((e = c->trace.ensure(1 << 16, false, s))) return e;
+  }
+  if ((e = ensure_pinned_counters(c, 1))) return e;
+  int grid = 0;
+  if ((e = grid_size(c->device, c->di, p.block_size, true, p.ctas_per_sm, &grid))) return e;
+
+  InstDesc d;
+  memset(&d, 0, sizeof(d));
+  d.row_ptr = row;
+  d.col = col;
+  d.w = w;
+  d.dist = dist;
+  d.update = update;
+  d.n = n;
+  d.m = (int32_t)m;
+  d.src = src;
+  d.mode = mode;
+  d.q[0] = c->q0.p;
+  d.q[1] = c->q1.p;
+  d.fq[0] = c->f0.p;
+  d.fq[1] = c->f1.p;
+  d.mark = c->mark.p;
+  d.fmark = c->fmark.p;
+  d.heavy = c->heavy.p;
+  d.qcap = (uint32_t)n;
+  d.hcap = hcap;
+  d.ctr = ctl.ctr();
+  d.stamp_base = c->stamp.p;
+  d.trace = p.trace ? c->trace.p : nullptr;
+  d.trace_cap = p.trace ? (uint32_t)c->trace.n : 0;
+  d.vec_ok = (((uintptr_t)col | (uintptr_t)w) & 15) == 0;
+  fill_thresholds(p, d);
+
+  TeamDesc td{0, grid, 0, 1};
+  // single-instance launches read the team table from a small device buffer
+  static_assert(sizeof(TeamDesc) == 16, "team descriptor layout");
+  LaunchParams lp;
+  memset(&lp, 0, sizeof(lp));
+  lp.inst = nullptr;
+  lp.order = nullptr;
+  lp.n_teams = 1;
+  lp.fault_inject_wait = p.reserved[0] != 0;
+  lp.bar = ctl.bar();
+  lp.abort_flag = ctl.abort_flag();
+  lp.timeout_ns = (unsigned long long)(p.timeout_s * 1e9);
+  lp.run_budget_ns = run_budget_ns(p);
+  lp.policy = policy_ptr(c->device);
+  if (p.policy == NPS_POLICY_LEARNED && !lp.policy)
+    return nps_fail(NPS_ERR_INVALID_ARG, "learned policy requested but no weights loaded (nps_policy_set_weights)");
+  // the team table lives after the abort flag in the control block
+  TeamDesc* d_team = (TeamDesc*)(ctl.abort_flag() + 16);
+  lp.teams = d_team;
+
+  NPS_CUDA(cudaMemsetAsync(ctl.base, 0, ctl.bytes - 128 + 64, s));
+  NPS_CUDA(cudaMemcpyAsync(d_team, &td, sizeof(td), cudaMemcpyHostToDevice, s));
+  if (time_it) NPS_CUDA(cudaEventRecord(c->ev[1], s));
+  if ((e = launch(c, s, p.block_size, true, grid, lp, d))) return e;
+  if (time_it) NPS_CUDA(cudaEventRecord(c->ev[2], s));
+  NPS_CUDA(cudaMemcpyAsync(c->h_ctr, ctl.ctr(), sizeof(Counters), cudaMemcpyDeviceToHost, s));
+  if (st) st->grid_ctas = grid;
+  return NPS_OK;
+}
+
+// A launch that stopped early never advanced its stamp base, so its stamps
+// could collide with the next run's: clear marks and base after any failure.
+void reset_stamps(nps_ctx* c, cudaStream_t s) {
+  if (c->mark.p) cudaMemsetAsync(c->mark.p, 0, c->mark.n * sizeof(uint32_t), s);
+  if (c->fmark.p) cudaMemsetAsync(c->fmark.p, 0, c->fmark.n * sizeof(uint32_t), s);
+  if (c->stamp.p) cudaMemsetAsync(c->stamp.p, 0, sizeof(uint32_t), s);
+  cudaStreamSynchronize(s);
+}
+
+void fill_stats(const Counters& k, nps_stats* st) {
+  if (!st) return;
+  st->iterations = k.iterations;
+  st->buckets = k.buckets;
+  st->edges_scanned = k.edges;
+  st->improvements = k.improvements;
+  st->vertices_processed = k.processed;
+  st->status = (int32_t)k.status;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+
+extern "C" nps_status nps_ctx_create(int32_t device, nps_ctx** out) {
+  if (!out) return nps_fail(NPS_ERR_INVALID_ARG, "ctx_create: null output");
+  auto* c = new nps_ctx();
+  nps_status st = ctx_init(c, device);
+  if (st != NPS_OK) {
+    ctx_release(c);
+    delete c;
+    return st;
+  }
+  *out = c;
+  return NPS_OK;
+}
+
+extern "C" nps_status nps_ctx_destroy(nps_ctx* ctx) {
+  if (!ctx) return NPS_OK;
+  ctx_release(ctx);
+  delete ctx;
+  return NPS_OK;
+}
+
+extern "C" nps_status nps_sssp_ctx(nps_ctx* c, const int32_t* row_ptr, const int32_t* col,
+                                   const uint32_t* w, int32_t n, int64_t m, int32_t src,
+                                   const nps_params* pin, uint32_t* dist_out, nps_stats* st) {
+  nps_clear_error();
+  nps_params p;
+  if (pin) p = *pin;
+  else nps_params_default(&p);
+  if (!c) return nps_fail(NPS_ERR_INVALID_ARG, "null context");
+  nps_status e = check_params(p);
+  if (e) return e;
+  if (n <= 0) return nps_fail(NPS_ERR_INVALID_ARG, "n must be positive");
+  if (m < 0 || m >= (int64_t)INT32_MAX) return nps_fail(NPS_ERR_INVALID_ARG, "m must be in [0, 2^31-1)");
+  if (src < 0 || src >= n) return nps_fail(NPS_ERR_INVALID_ARG, "source vertex out of range");
+  if (!row_ptr || !dist_out || (m > 0 && (!col || !w))) return nps_fail(NPS_ERR_INVALID_ARG, "null array");
+  std::lock_guard<std::mutex> lk(c->mu);
+  NPS_CUDA(cudaSetDevice(c->device));
+  cudaStream_t s = p.stream ? (cudaStream_t)p.stream : c->stream;
+  if (st) memset(st, 0, sizeof(*st));
+
+  const int32_t *drow = row_ptr, *dcol = col;
+  const uint32_t* dw = w;
+  uint32_t* ddist = dist_out;
+  NPS_CUDA(cudaEventRecord(c->ev[0], s));
+  if (!p.device_ptrs) {
+    // host arrays: validate the CSR shape on the host, then stage on the device
+    if (row_ptr[0] != 0 || row_ptr[n] != (int32_t)m)
+      return nps_fail(NPS_ERR_FORMAT, "malformed CSR: row_ptr[0] must be 0 and row_ptr[n] must be m");
+    if ((e = c->g_row.ensure((size_t)n + 1, false, s)) || (e = c->g_col.ensure((size_t)m, false, s)) ||
+        (e = c->g_w.ensure((size_t)m, false, s)) || (e = c->g_dist.ensure((size_t)n, false, s)))
+      return e;
+    NPS_CUDA(cudaMemcpyAsync(c->g_row.p, row_ptr, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, s));
+    if (m > 0) {
+      NPS_CUDA(cudaMemcpyAsync(c->g_col.p, col, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
+      NPS_CUDA(cudaMemcpyAsync(c->g_w.p, w, sizeof(uint32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
+    }
+    drow = c->g_row.p;
+    dcol = c->g_col.p;
+    dw = c->g_w.p;
+    ddist = c->g_dist.p;
+  }
+  if ((e = run_single(c, s, drow, dcol, dw, n, m, src, ddist, nullptr, 0, p, st, true))) return e;
+  if (!p.device_ptrs)
+    NPS_CUDA(cudaMemcpyAsync(dist_out, ddist, sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToHost, s));
+  NPS_CUDA(cudaEventRecord(c->ev[3], s));
+  NPS_CUDA(cudaStreamSynchronize(s));
+  const Counters& k = *c->h_ctr;
+  c->trace_count = p.trace ? std::min<uint32_t>(k.iterations, (uint32_t)c->trace.n) : 0;
+  if (st) {
+    fill_stats(k, st);
+    cudaEventElapsedTime(&st->kernel_ms, c->ev[1], c->ev[2]);
+    cudaEventElapsedTime(&st->total_ms, c->ev[0], c->ev[3]);
+    st->reached = k.reached + 1;
+  }
+  if (k.status) reset_stamps(c, s);
+  return status_from_device(k.status);
+}
+
+extern "C" nps_status nps_sssp(const int32_t* row_ptr, const int32_t* col, const uint32_t* w, int32_t n,
+                               int64_t m, int32_t src, const nps_params* p, uint32_t* dist_out,
+                               nps_stats* st) {
+  nps_clear_error();
+  nps_ctx* c = nullptr;
+  nps_status e = default_ctx(p ? p->device : 0, &c);
+  if (e) return e;
+  return nps_sssp_ctx(c, row_ptr, col, w, n, m, src, p, dist_out, st);
+}
+
+extern "C" nps_status nps_sssp_state(const int32_t* d_row_ptr, const int32_t* d_col, const uint32_t* d_w,
+                                     int32_t n, int64_t m, uint32_t* d_cost, uint8_t* d_update,
+                                     const nps_params* pin, nps_stats* st) {
+  nps_clear_error();
+  nps_params p;
+  if (pin) p = *pin;
+  else nps_params_default(&p);
+  nps_status e = check_params(p);
+  if (e) return e;
+  if (n <= 0) return nps_fail(NPS_ERR_INVALID_ARG, "n must be positive");
+  if (m < 0 || m >= (int64_t)INT32_MAX) return nps_fail(NPS_ERR_INVALID_ARG, "m must be in [0, 2^31-1)");
+  if (!d_row_ptr || !d_cost || !d_update || (m > 0 && (!d_col || !d_w)))
+    return nps_fail(NPS_ERR_INVALID_ARG, "null array");
+  nps_ctx* c = nullptr;
+  if ((e = default_ctx(p.device, &c))) return e;
+  std::lock_guard<std::mutex> lk(c->mu);
+  NPS_CUDA(cudaSetDevice(c->device));
+  cudaStream_t s = p.stream ? (cudaStream_t)p.stream : c->stream;
+  if (st) memset(st, 0, sizeof(*st));
+  NPS_CUDA(cudaEventRecord(c->ev[0], s));
+  if ((e = run_single(c, s, d_row_ptr, d_col, d_w, n, m, 0, d_cost, d_update, 1, p, st, true))) return e;
+  NPS_CUDA(cudaEventRecord(c->ev[3], s));
+  NPS_CUDA(cudaStreamSynchronize(s));
+  const Counters& k = *c->h_ctr;
+  c->trace_count = p.trace ? std::min<uint32_t>(k.iterations, (uint32_t)c->trace.n) : 0;
+  if (st) {
+    fill_stats(k, st);
+    cudaEventElapsedTime(&st->kernel_ms, c->ev[1], c->ev[2]);
+    cudaEventElapsedTime(&st->total_ms, c->ev[0], c->ev[3]);
+    st->reached = k.reached;
+  }
+  if (k.status) reset_stamps(c, s);
+  return status_from_device(k.status);
+}
+
+extern "C" nps_status nps_trace_read(int32_t device, nps_trace_rec* out, int32_t cap, int32_t* count) {
+  nps_clear_error();
+  if (!out || !count || cap < 0) return nps_fail(NPS_ERR_INVALID_ARG, "trace_read: bad argument");
+  nps_ctx* c = nullptr;
+  nps_status e = default_ctx(device, &c);
+  if (e) return e;
+  std::lock_guard<std::mutex> lk(c->mu);
+  NPS_CUDA(cudaSetDevice(c->device));
+  int32_t k = (int32_t)std::min<uint32_t>(c->trace_count, (uint32_t)cap);
+  if (k > 0) NPS_CUDA(cudaMemcpy(out, c->trace.p, sizeof(nps_trace_rec) * (size_t)k, cudaMemcpyDeviceToHost));
+  *count = k;
+  return NPS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// batch
+
+extern "C" nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, const nps_params* pin,
+                                     int32_t use_graph, nps_stats* per_instance, float* kernel_ms) {
+  nps_clear_error();
+  nps_params p;
+  if (pin) p = *pin;
+  else nps_params_default(&p);
+  nps_status e = check_params(p);
+  if (e) return e;
+  if (!inst || count <= 0 || count > 65536) return nps_fail(NPS_ERR_INVALID_ARG, "batch: need 1..65536 instances");
+  for (int i = 0; i < count; ++i) {
+    const nps_instance& x = inst[i];
+    if (x.n <= 0 || x.m < 0 || x.m >= (int64_t)INT32_MAX || x.src < 0 || x.src >= x.n || !x.row_ptr || !x.dist ||
+        (x.m > 0 && (!x.col || !x.w)))
+      return nps_fail(NPS_ERR_INVALID_ARG, "batch: instance " + std::to_string(i) + " is invalid");
+  }
+  nps_ctx* c = nullptr;
+  if ((e = default_ctx(p.device, &c))) return e;
+  std::lock_guard<std::mutex> lk(c->mu);
+  NPS_CUDA(cudaSetDevice(c->device));
+  cudaStream_t s = p.stream ? (cudaStream_t)p.stream : c->stream;
+  int grid = 0;
+  if ((e = grid_size(c->device, c->di, p.block_size, false, p.ctas_per_sm, &grid))) return e;
+
+  const bool same = c->b_graph && (int)c->b_key.size() == count && c->b_grid == grid && c->b_bs == p.block_size &&
+                    memcmp(c->b_key.data(), inst, sizeof(nps_instance) * count) == 0 &&
+                    memcmp(&c->b_params_key, &p, sizeof(p)) == 0;
+  const int nteams = std::min(count, grid);
+  Control ctl;
+  ctl.n_inst = (size_t)count;
+  ctl.n_teams = (size_t)nteams;
+  ctl.bytes = sizeof(Counters) * (size_t)count + 32 * sizeof(uint32_t) * (size_t)nteams + 128;
+
+  if (!same) {
+    if (c->b_graph) cudaGraphExecDestroy(c->b_graph);
+    c->b_graph = nullptr;
+    // workspace: per instance 4 queues of n int32 + marks carved from pools
+    size_t q_total = 0, h_total = 0;
+    std::vector<uint32_t> hcap(count);
+    for (int i = 0; i < count; ++i) {
+      q_total += 4 * (size_t)inst[i].n;
+      hcap[i] = heavy_capacity(inst[i].n, inst[i].m, p);
+      h_total += hcap[i];
+    }
+    size_t mk_total = 0;
+    for (int i = 0; i < count; ++i) mk_total += 2 * (size_t)inst[i].n;
+    if ((e = c->b_pool.ensure(q_total, false, s))) return e;
+    const bool regrow = c->b_stamp.n < mk_total + (size_t)count;
+    if ((e = c->b_stamp.ensure(mk_total + (size_t)count, true, s))) return e;
+    if (!regrow) NPS_CUDA(cudaMemsetAsync(c->b_stamp.p, 0, sizeof(uint32_t) * (mk_total + count), s));
+    if ((e = c->b_heavy.ensure(h_total, false, s))) return e;
+    if ((e = c->b_control.ensure(ctl.bytes, false, s))) return e;
+    if ((e = c->b_inst.ensure((size_t)count, false, s))) return e;
+    if ((e = c->b_teams.ensure((size_t)nteams, false, s))) return e;
+    if ((e = c->b_order.ensure((size_t)count, false, s))) return e;
+    ctl.base = c->b_control.p;
+
+    // team formation: longest-processing-time assignment of instances to
+    // nteams teams by work (m + n), then CTAs proportional to team work
+    std::vector<int> idx(count);
+    for (int i = 0; i < count; ++i) idx[i] = i;
+    auto work = [&](int i) { return (double)inst[i].m + (double)inst[i].n; };
+    std::sort(idx.begin(), idx.end(), [&](int a, int b) { return work(a) > work(b) || (work(a) == work(b) && a < b); });
+    std::vector<double> tw(nteams, 0.0);
+    std::vector<std::vector<int>> members(nteams);
+    for (int i : idx) {
+      int t = (int)(std::min_element(tw.begin(), tw.end()) - tw.begin());
+      tw[t] += work(i);
+      members[t].push_back(i);
+    }
+    double total = 0;
+    for (double x : tw) total += x;
+    std::vector<int> ctas(nteams, 1);
+    int left = grid - nteams;
+    std::vector<std::pair<double, int>> frac;
+    for (int t = 0; t < nteams; ++t) {
+      double want = total > 0 ? (double)(grid)*tw[t] / total : (double)grid / nteams;
+      int extra = std::max(0, (int)std::floor(want) - 1);
+      extra = std::min(extra, left);
+      ctas[t] += extra;
+      left -= extra;
+      frac.push_back({want - std::floor(want), t});
+    }
+    std::sort(frac.begin(), frac.end(), [](auto& a, auto& b) { return a.first > b.first; });
+    for (size_t k = 0; left > 0 && k < frac.size(); ++k, --left) ctas[frac[k].second]++;
+    std::vector<TeamDesc> teams(nteams);
+    std::vector<int32_t> order;
+    int cb = 0;
+    for (int t = 0; t < nteams; ++t) {
+      teams[t].cta_begin = cb;
+      teams[t].cta_count = ctas[t];
+      teams[t].inst_begin = (int32_t)order.size();
+      teams[t].inst_count = (int32_t)members[t].size();
+      for (int i : members[t]) order.push_back(i);
+      cb += ctas[t];
+    }
+    // descriptors
+    c->b_inst_host.assign(count, InstDesc{});
+    size_t qo = 0, ho = 0, mo = 0;
+    uint32_t* stamps = c->b_stamp.p + mk_total;
+    for (int i = 0; i < count; ++i) {
+      InstDesc& d = c->b_inst_host[i];
+      memset(&d, 0, sizeof(d));
+      const nps_instance& x = inst[i];
+      d.row_ptr = x.row_ptr;
+      d.col = x.col;
+      d.w = x.w;
+      d.dist = x.dist;
+      d.n = x.n;
+      d.m = (int32_t)x.m;
+      d.src = x.src;
+      d.mode = 0;
+      for (int k = 0; k < 2; ++k) {
+        d.q[k] = c->b_pool.p + qo;
+        qo += x.n;
+        d.fq[k] = c->b_pool.p + qo;
+        qo += x.n;
+      }
+      d.mark = c->b_stamp.p + mo;
+      mo += x.n;
+      d.fmark = c->b_stamp.p + mo;
+      mo += x.n;
+      d.heavy = c->b_heavy.p + ho;
+      d.hcap = hcap[i];
+      ho += hcap[i];
+      d.qcap = (uint32_t)x.n;
+      d.ctr = ctl.ctr() + i;
+      d.stamp_base = stamps + i;
+      d.vec_ok = (((uintptr_t)x.col | (uintptr_t)x.w) & 15) == 0;
+      fill_thresholds(p, d);
+    }
+    NPS_CUDA(cudaMemcpyAsync(c->b_inst.p, c->b_inst_host.data(), sizeof(InstDesc) * count, cudaMemcpyHostToDevice, s));
+    NPS_CUDA(cudaMemcpyAsync(c->b_teams.p, teams.data(), sizeof(TeamDesc) * nteams, cudaMemcpyHostToDevice, s));
+    NPS_CUDA(cudaMemcpyAsync(c->b_order.p, order.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice, s));
+    NPS_CUDA(cudaStreamSynchronize(s));  // host vectors above go out of scope
+    c->b_key.assign(inst, inst + count);
+    c->b_params_key = p;
+    c->b_grid = grid;
+    c->b_bs = p.block_size;
+    c->b_nteams = nteams;
+  }
+  ctl.base = c->b_control.p;
+  LaunchParams lp;
+  memset(&lp, 0, sizeof(lp));
+  lp.inst = c->b_inst.p;
+  lp.order = c->b_order.p;
+  lp.teams = c->b_teams.p;
+  lp.n_teams = c->b_nteams;
+  lp.fault_inject_wait = p.reserved[0] != 0;
+  lp.bar = ctl.bar();
+  lp.abort_flag = ctl.abort_flag();
+  lp.timeout_ns = (unsigned long long)(p.timeout_s * 1e9);
+  lp.run_budget_ns = run_budget_ns(p);
+  lp.policy = policy_ptr(c->device);
+  if (p.policy == NPS_POLICY_LEARNED && !lp.policy)
+    return nps_fail(NPS_ERR_INVALID_ARG, "learned policy requested but no weights loaded (nps_policy_set_weights)");
+  InstDesc dummy;
+  memset(&dummy, 0, sizeof(dummy));
+  if ((e = ensure_pinned_counters(c, (size_t)count))) return e;
+
+  NPS_CUDA(cudaEventRecord(c->ev[1], s));
+  if (use_graph) {
+    if (!c->b_graph) {
+      cudaGraph_t g = nullptr;
+      NPS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      cudaError_t ce = cudaMemsetAsync(ctl.base, 0, ctl.bytes - 64, s);
+      nps_status le = ce == cudaSuccess ? launch(c, s, p.block_size, false, grid, lp, dummy) : NPS_ERR_CUDA;
+      cudaError_t ee = cudaStreamEndCapture(s, &g);
+      if (ce != cudaSuccess) return nps_fail(NPS_ERR_CUDA, std::string("capture memset: ") + cudaGetErrorString(ce));
+      if (le) {
+        if (g) cudaGraphDestroy(g);
+        return le;
+      }
+      if (ee != cudaSuccess) return nps_fail(NPS_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ee));
+      cudaError_t ie = cudaGraphInstantiate(&c->b_graph, g, 0);
+      cudaGraphDestroy(g);
+      if (ie != cudaSuccess) {
+        c->b_graph = nullptr;
+        return nps_fail(NPS_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ie));
+      }
+      NPS_CUDA(cudaEventRecord(c->ev[1], s));
+    }
+    NPS_CUDA(cudaGraphLaunch(c->b_graph, s));
+  } else {
+    NPS_CUDA(cudaMemsetAsync(ctl.base, 0, ctl.bytes - 64, s));
+    if ((e = launch(c, s, p.block_size, false, grid, lp, dummy))) return e;
+  }
+  NPS_CUDA(cudaEventRecord(c->ev[2], s));
+  NPS_CUDA(cudaMemcpyAsync(c->h_ctr, ctl.ctr(), sizeof(Counters) * count, cudaMemcpyDeviceToHost, s));
+  NPS_CUDA(cudaStreamSynchronize(s));
+  if (kernel_ms) cudaEventElapsedTime(kernel_ms, c->ev[1], c->ev[2]);
+  uint32_t first_err = 0;
+  for (int i = 0; i < count; ++i) {
+    const Counters& k = c->h_ctr[i];
+    if (per_instance) {
+      memset(&per_instance[i], 0, sizeof(nps_stats));
+      fill_stats(k, &per_instance[i]);
+      per_instance[i].reached = k.reached + 1;
+      per_instance[i].grid_ctas = grid;
+    }
+    if (k.status && !first_err) first_err = k.status;
+  }
+  if (first_err) {  // stamps of an aborted batch may collide with the next run's
+    cudaMemsetAsync(c->b_stamp.p, 0, c->b_stamp.n * sizeof(uint32_t), s);
+    cudaStreamSynchronize(s);
+  }
+  return status_from_device(first_err);
+}
+
+// ---------------------------------------------------------------------------
+// policy weights
+
+extern "C" nps_status nps_policy_set_weights(int32_t device, const float* w1, const float* b1, const float* w2,
+                                             const float* b2, const float* mean, const float* istd) {
+  nps_clear_error();
+  if (!w1 || !b1 || !w2 || !b2 || !mean || !istd) return nps_fail(NPS_ERR_INVALID_ARG, "policy: null array");
+  DevInfo di;
+  nps_status e = device_info(device, &di);
+  if (e) return e;
+  PolicyDev h;
+  memset(&h, 0, sizeof(h));
+  auto to_bf16 = [](float f) -> uint16_t {  // round to nearest even
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    if ((u & 0x7f800000u) == 0x7f800000u) return (uint16_t)(u >> 16);
+    u += 0x7fffu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+  };
+  for (int i = 0; i < NPS_MLP_HID * NPS_MLP_IN; ++i) h.w1[i] = to_bf16(w1[i]);
+  for (int i = 0; i < NPS_MLP_OUT * NPS_MLP_HID; ++i) h.w2[i] = to_bf16(w2[i]);
+  memcpy(h.b1, b1, sizeof(h.b1));
+  memcpy(h.b2, b2, sizeof(h.b2));
+  memcpy(h.mean, mean, sizeof(h.mean));
+  memcpy(h.istd, istd, sizeof(h.istd));
+  std::lock_guard<std::mutex> lk(g_policy_mu);
+  if ((int)g_policy.size() <= device) g_policy.resize(device + 1);
+  NPS_CUDA(cudaSetDevice(device));
+  if (!g_policy[device].dev) NPS_CUDA(cudaMalloc(&g_policy[device].dev, sizeof(PolicyDev)));
+  NPS_CUDA(cudaMemcpy(g_policy[device].dev, &h, sizeof(h), cudaMemcpyHostToDevice));
+  g_policy[device].set = true;
+  return NPS_OK;
+}

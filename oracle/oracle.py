@@ -1,0 +1,168 @@
+"""Python loader of the SSSP oracle -- TEST INFRASTRUCTURE ONLY.
+
+Imported by tests/, __graft_entry__.smoke() and the cpu_baseline / reference
+legs of bench.py, always as the checker or the timed CPU baseline.  The library
+in nested-parallelism_b200/ never imports it.
+
+  liboracle.so          C restatement (sssp_oracle.c): heap Dijkstra, d-heap
+                        Dijkstra, state fixpoint
+  _ref/libref_sssp.so   the reference's own SSSP_CPU / usssp_cpu / dheap built
+                        from its sources by oracle/Makefile (absent if the
+                        reference tree was not available when it was built)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libref_sssp.so")
+INF = 0x40000000
+
+_P, _I32, _I64, _D = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+
+_orc = None
+_ref = None
+
+
+def _load_oracle():
+    global _orc
+    if _orc is None:
+        if not os.path.exists(ORACLE_SO):
+            raise ImportError(f"{ORACLE_SO} missing: run `make -C {HERE}`")
+        lib = C.CDLL(ORACLE_SO)
+        lib.oracle_sssp_heap.argtypes = [_I32, _P, _P, _P, _I32, _P]
+        lib.oracle_sssp_heap.restype = C.c_int
+        lib.oracle_sssp_dheap.argtypes = [_I32, _P, _P, _P, _I32, C.c_int, _P]
+        lib.oracle_sssp_dheap.restype = C.c_int
+        lib.oracle_sssp_state.argtypes = [_I32, _P, _P, _P, _P, _P]
+        lib.oracle_sssp_state.restype = C.c_int
+        lib.oracle_reached.argtypes = [_I32, _P, _P, C.POINTER(_I64), C.POINTER(_I64)]
+        lib.oracle_reached.restype = None
+        lib.oracle_fnv1a_u32.argtypes = [_P, _I64]
+        lib.oracle_fnv1a_u32.restype = C.c_uint64
+        _orc = lib
+    return _orc
+
+
+def have_reference() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def _load_ref():
+    global _ref
+    if _ref is None:
+        if not have_reference():
+            raise ImportError(f"{REF_SO} missing: the reference CPU code was not built")
+        lib = C.CDLL(REF_SO)
+        lib.nps_ref_sssp_cpu.argtypes = [_I32, _I32, _P, _P, _P, _I32, _P]
+        lib.nps_ref_sssp_cpu.restype = _D
+        lib.nps_ref_heap_init_seconds.argtypes = []
+        lib.nps_ref_heap_init_seconds.restype = _D
+        lib.nps_ref_usssp_cpu.argtypes = [_I32, _I32, _P, _P, _P, _I32, _I32, _P]
+        lib.nps_ref_usssp_cpu.restype = _D
+        lib.nps_ref_dijkstra_dheap.argtypes = [_I32, _P, _P, _P, _I32, _I32, _P]
+        lib.nps_ref_dijkstra_dheap.restype = _D
+        _ref = lib
+    return _ref
+
+
+def _arrs(row, col, w):
+    return (np.ascontiguousarray(row, dtype=np.int32), np.ascontiguousarray(col, dtype=np.int32),
+            np.ascontiguousarray(w, dtype=np.uint32))
+
+
+def sssp_heap(row, col, w, src):
+    """Restated SSSP_CPU (lazy binary-heap Dijkstra)."""
+    row, col, w = _arrs(row, col, w)
+    n = row.shape[0] - 1
+    d = np.empty(n, dtype=np.uint32)
+    rc = _load_oracle().oracle_sssp_heap(n, row.ctypes.data, col.ctypes.data, w.ctypes.data, int(src),
+                                         d.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"oracle_sssp_heap failed ({rc})")
+    return d
+
+
+def sssp_dheap(row, col, w, src, d=4):
+    """Restated d-ary-heap Dijkstra with decrease-key (dheap API)."""
+    row, col, w = _arrs(row, col, w)
+    n = row.shape[0] - 1
+    out = np.empty(n, dtype=np.uint32)
+    rc = _load_oracle().oracle_sssp_dheap(n, row.ctypes.data, col.ctypes.data, w.ctypes.data, int(src), int(d),
+                                          out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"oracle_sssp_dheap failed ({rc})")
+    return out
+
+
+def sssp_state(row, col, w, cost, update):
+    """Label-correcting fixpoint from a cost / update state (returns new arrays)."""
+    row, col, w = _arrs(row, col, w)
+    n = row.shape[0] - 1
+    c = np.array(cost, dtype=np.uint32, copy=True)
+    u = np.array(update, dtype=np.uint8, copy=True)
+    rc = _load_oracle().oracle_sssp_state(n, row.ctypes.data, col.ctypes.data, w.ctypes.data, c.ctypes.data,
+                                          u.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"oracle_sssp_state failed ({rc})")
+    return c, u
+
+
+def reached(row, dist):
+    row = np.ascontiguousarray(row, dtype=np.int32)
+    dist = np.ascontiguousarray(dist, dtype=np.uint32)
+    a, b = _I64(0), _I64(0)
+    _load_oracle().oracle_reached(row.shape[0] - 1, row.ctypes.data, dist.ctypes.data, C.byref(a), C.byref(b))
+    return int(a.value), int(b.value)
+
+
+def fnv1a(dist) -> int:
+    a = np.ascontiguousarray(dist, dtype=np.uint32)
+    return int(_load_oracle().oracle_fnv1a_u32(a.ctypes.data, a.shape[0]))
+
+
+# ---- the reference's own code --------------------------------------------
+
+def ref_sssp_cpu(row, col, w, src):
+    """The reference's SSSP_CPU() on these arrays; returns (dist uint32, seconds)."""
+    row, col, w = _arrs(row, col, w)
+    n, m = row.shape[0] - 1, col.shape[0]
+    cost = np.empty(n, dtype=np.int32)
+    t = _load_ref().nps_ref_sssp_cpu(n, m, row.ctypes.data, col.ctypes.data, w.ctypes.data, int(src),
+                                     cost.ctypes.data)
+    return cost.view(np.uint32), float(t)
+
+
+def ref_heap_init_seconds() -> float:
+    return float(_load_ref().nps_ref_heap_init_seconds())
+
+
+def ref_usssp_cpu(row, col, w, src, threads=0):
+    """The reference's OpenMP frontier sweep (racy, not exact with >1 thread)."""
+    row, col, w = _arrs(row, col, w)
+    n, m = row.shape[0] - 1, col.shape[0]
+    cost = np.empty(n, dtype=np.int32)
+    t = _load_ref().nps_ref_usssp_cpu(n, m, row.ctypes.data, col.ctypes.data, w.ctypes.data, int(src),
+                                      int(threads), cost.ctypes.data)
+    return cost.view(np.uint32), float(t)
+
+
+def ref_dijkstra_dheap(row, col, w, src, d=2):
+    """Dijkstra with decrease-key on the reference's dheap class."""
+    row, col, w = _arrs(row, col, w)
+    n = row.shape[0] - 1
+    cost = np.empty(n, dtype=np.int32)
+    t = _load_ref().nps_ref_dijkstra_dheap(n, row.ctypes.data, col.ctypes.data, w.ctypes.data, int(src), int(d),
+                                           cost.ctypes.data)
+    return cost.view(np.uint32), float(t)
+
+
+def timed(fn, *a, **k):
+    t0 = time.perf_counter()
+    r = fn(*a, **k)
+    return r, time.perf_counter() - t0

@@ -1,0 +1,269 @@
+/*
+ * sssp_oracle.c -- CPU oracle for the SSSP hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker: only tests/, the smoke
+ * check in __graft_entry__.py and the cpu_baseline / reference legs of bench.py
+ * load it.  The library (nested-parallelism_b200/) never links or calls it, and
+ * has no CPU fallback.
+ *
+ * Restated algorithms (paths relative to the dadaism/nested-parallelism tree):
+ *
+ *   oracle_sssp_heap   SSSP_CPU() in apps/sssp/src/cpu/sssp.cpp:13-47 on the
+ *                      Heap class of common/heap.cpp:29-109: lazy-insertion
+ *                      binary-heap Dijkstra.  Pop (id, key); if cost[id] is still
+ *                      INF, settle it with key and insert (nid, key + w) for every
+ *                      out-edge whose head is unsettled (sssp.cpp:29-41).
+ *   oracle_sssp_dheap  Dijkstra with decrease-key on a d-ary heap with the item /
+ *                      key API of common/dheap.h:55-78 (items 1..N, insert,
+ *                      changekey, deletemin, member); the reference ships the heap
+ *                      with no SSSP driver, so the driver is written here.
+ *   oracle_sssp_state  the label-correcting fixpoint that sssp_np_consolidate_gpu()
+ *                      computes from an arbitrary cost[] / update[] state
+ *                      (apps/sssp/src/gpu/sssp_wrapper.cu:475-546 with the
+ *                      relaxation of sssp_kernel.cu:49-52), as a FIFO worklist.
+ *
+ * Distances are uint32 with INF = 2^30 (sssp_wrapper.cu:7, common/global.h:19).
+ * A tentative distance that reaches 2^30 is treated as unreachable; the
+ * reference's int arithmetic never gets there on the inputs it is run on.
+ *
+ * Pinned by tests/golden/: goldens produced by running the reference's own
+ * SSSP_CPU (compiled from its sources by oracle/Makefile into oracle/_ref/).
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ORACLE_INF 0x40000000u
+
+typedef struct {
+  uint32_t key;
+  int32_t id;
+} hitem;
+
+/* binary min-heap on key (ties in any order: they do not change distances) */
+typedef struct {
+  hitem* a;
+  int64_t n, cap;
+} bheap;
+
+static int bheap_push(bheap* h, uint32_t key, int32_t id) {
+  if (h->n == h->cap) {
+    int64_t nc = h->cap ? 2 * h->cap : 1024;
+    hitem* na = (hitem*)realloc(h->a, (size_t)nc * sizeof(hitem));
+    if (!na) return -1;
+    h->a = na;
+    h->cap = nc;
+  }
+  int64_t i = h->n++;
+  while (i > 0) {
+    int64_t p = (i - 1) >> 1;
+    if (h->a[p].key <= key) break;
+    h->a[i] = h->a[p];
+    i = p;
+  }
+  h->a[i].key = key;
+  h->a[i].id = id;
+  return 0;
+}
+
+static hitem bheap_pop(bheap* h) {
+  hitem top = h->a[0];
+  hitem last = h->a[--h->n];
+  int64_t i = 0;
+  for (;;) {
+    int64_t l = 2 * i + 1, r = l + 1, c = i;
+    uint32_t ck = last.key;
+    if (l < h->n && h->a[l].key < ck) {
+      c = l;
+      ck = h->a[l].key;
+    }
+    if (r < h->n && h->a[r].key < ck) c = r;
+    if (c == i) break;
+    h->a[i] = h->a[c];
+    i = c;
+  }
+  if (h->n > 0) h->a[i] = last;
+  return top;
+}
+
+/* Returns 0 on success, -1 on bad arguments, -2 on allocation failure. */
+int oracle_sssp_heap(int32_t n, const int32_t* row, const int32_t* col, const uint32_t* w, int32_t src,
+                     uint32_t* dist) {
+  if (n <= 0 || src < 0 || src >= n || !row || !dist) return -1;
+  for (int32_t i = 0; i < n; ++i) dist[i] = ORACLE_INF;
+  bheap h = {0, 0, 0};
+  if (bheap_push(&h, 0u, src)) return -2;
+  while (h.n > 0) {
+    hitem it = bheap_pop(&h);
+    if (dist[it.id] != ORACLE_INF) continue; /* already settled: lazy deletion */
+    dist[it.id] = it.key;
+    for (int32_t e = row[it.id]; e < row[it.id + 1]; ++e) {
+      int32_t v = col[e];
+      if (dist[v] != ORACLE_INF) continue;
+      uint64_t nd = (uint64_t)it.key + w[e];
+      if (nd >= ORACLE_INF) continue;
+      if (bheap_push(&h, (uint32_t)nd, v)) {
+        free(h.a);
+        return -2;
+      }
+    }
+  }
+  free(h.a);
+  return 0;
+}
+
+/* d-ary heap over items 1..N with positions and keys (the dheap.h layout):
+ * parent(x) = (x + d - 2) / d, children d(x-1)+2 .. dx+1. */
+typedef struct {
+  int d;
+  int64_t n;
+  int64_t* h;   /* h[1..n] items */
+  int64_t* pos; /* pos[item], 0 = absent */
+  uint64_t* key;
+} dheap;
+
+static void dh_siftup(dheap* H, int64_t i, int64_t x) {
+  while (x > 1) {
+    int64_t px = (x + H->d - 2) / H->d;
+    if (H->key[H->h[px]] <= H->key[i]) break;
+    H->h[x] = H->h[px];
+    H->pos[H->h[x]] = x;
+    x = px;
+  }
+  H->h[x] = i;
+  H->pos[i] = x;
+}
+
+static int64_t dh_minchild(dheap* H, int64_t x) {
+  int64_t first = (int64_t)H->d * (x - 1) + 2;
+  if (first > H->n) return 0;
+  int64_t last = (int64_t)H->d * x + 1, mc = first;
+  for (int64_t y = first + 1; y <= last && y <= H->n; ++y)
+    if (H->key[H->h[y]] < H->key[H->h[mc]]) mc = y;
+  return mc;
+}
+
+static void dh_siftdown(dheap* H, int64_t i, int64_t x) {
+  int64_t cx = dh_minchild(H, x);
+  while (cx != 0 && H->key[H->h[cx]] < H->key[i]) {
+    H->h[x] = H->h[cx];
+    H->pos[H->h[x]] = x;
+    x = cx;
+    cx = dh_minchild(H, x);
+  }
+  H->h[x] = i;
+  H->pos[i] = x;
+}
+
+int oracle_sssp_dheap(int32_t n, const int32_t* row, const int32_t* col, const uint32_t* w, int32_t src, int d,
+                      uint32_t* dist) {
+  if (n <= 0 || src < 0 || src >= n || !row || !dist || d < 2) return -1;
+  dheap H;
+  H.d = d;
+  H.n = 0;
+  H.h = (int64_t*)malloc(sizeof(int64_t) * ((size_t)n + 1));
+  H.pos = (int64_t*)calloc((size_t)n + 1, sizeof(int64_t));
+  H.key = (uint64_t*)malloc(sizeof(uint64_t) * ((size_t)n + 1));
+  char* done = (char*)calloc((size_t)n, 1);
+  if (!H.h || !H.pos || !H.key || !done) {
+    free(H.h);
+    free(H.pos);
+    free(H.key);
+    free(done);
+    return -2;
+  }
+  for (int32_t i = 0; i < n; ++i) dist[i] = ORACLE_INF;
+  dist[src] = 0;
+  /* insert: item = vertex + 1 */
+  H.key[src + 1] = 0;
+  H.n = 1;
+  dh_siftup(&H, src + 1, 1);
+  while (H.n > 0) {
+    int64_t it = H.h[1];
+    /* deletemin: move the last item into the root position */
+    int64_t j = H.h[H.n--];
+    if (it != j) dh_siftdown(&H, j, 1);
+    H.pos[it] = 0;
+    int32_t u = (int32_t)(it - 1);
+    done[u] = 1;
+    for (int32_t e = row[u]; e < row[u + 1]; ++e) {
+      int32_t v = col[e];
+      if (done[v]) continue;
+      uint64_t nd = (uint64_t)dist[u] + w[e];
+      if (nd >= ORACLE_INF || nd >= dist[v]) continue;
+      dist[v] = (uint32_t)nd;
+      H.key[v + 1] = nd;
+      if (H.pos[v + 1]) {
+        dh_siftup(&H, v + 1, H.pos[v + 1]); /* changekey to a smaller key */
+      } else {
+        H.n++;
+        dh_siftup(&H, v + 1, H.n);
+      }
+    }
+  }
+  free(H.h);
+  free(H.pos);
+  free(H.key);
+  free(done);
+  return 0;
+}
+
+/* Label-correcting fixpoint from a state: cost[] is updated in place, update[]
+ * flags the initial frontier and is cleared.  FIFO worklist with an in-queue flag. */
+int oracle_sssp_state(int32_t n, const int32_t* row, const int32_t* col, const uint32_t* w, uint32_t* cost,
+                      uint8_t* update) {
+  if (n <= 0 || !row || !cost || !update) return -1;
+  int32_t* q = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
+  char* inq = (char*)calloc((size_t)n, 1);
+  if (!q || !inq) {
+    free(q);
+    free(inq);
+    return -2;
+  }
+  int64_t head = 0, count = 0;
+  for (int32_t v = 0; v < n; ++v)
+    if (update[v]) {
+      update[v] = 0;
+      q[(head + count++) % n] = v;
+      inq[v] = 1;
+    }
+  while (count > 0) {
+    int32_t u = q[head];
+    head = (head + 1) % n;
+    count--;
+    inq[u] = 0;
+    uint32_t du = cost[u];
+    if (du >= ORACLE_INF) continue;
+    for (int32_t e = row[u]; e < row[u + 1]; ++e) {
+      int32_t v = col[e];
+      uint64_t nd = (uint64_t)du + w[e];
+      if (nd >= ORACLE_INF || nd >= cost[v]) continue;
+      cost[v] = (uint32_t)nd;
+      if (!inq[v]) {
+        inq[v] = 1;
+        q[(head + count++) % n] = v;
+      }
+    }
+  }
+  free(q);
+  free(inq);
+  return 0;
+}
+
+/* Out-edges of reached vertices (m_r) and reached-vertex count (n_r). */
+void oracle_reached(int32_t n, const int32_t* row, const uint32_t* dist, int64_t* n_r, int64_t* m_r) {
+  int64_t a = 0, b = 0;
+  for (int32_t v = 0; v < n; ++v)
+    if (dist[v] < ORACLE_INF) {
+      a++;
+      b += row[v + 1] - row[v];
+    }
+  *n_r = a;
+  *m_r = b;
+}
+
+uint64_t oracle_fnv1a_u32(const uint32_t* a, int64_t n) {
+  uint64_t h = 1469598103934665603ull;
+  for (int64_t i = 0; i < n; ++i) h = (h ^ (uint64_t)a[i]) * 1099511628211ull;
+  return h;
+}
