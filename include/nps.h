@@ -116,7 +116,8 @@ typedef struct nps_trace_rec {
   uint64_t edges;           /* edges scanned in the iteration */
   uint64_t improvements;
   uint32_t reached;         /* vertices reached so far */
-  uint32_t pad;
+  uint32_t heavy;           /* grid-tier rows collected for the next iteration */
+  uint64_t t_ns;            /* device time since the launch began, at the end of the iteration */
 } nps_trace_rec;
 
 /* Host-side CSR graph, library-allocated; free with nps_graph_free. */

@@ -11,7 +11,7 @@
 //     (sssp_kernel.cu:330-541), which buffer vertices of degree >= THRESHOLD per
 //     warp / block / grid and launch a dynamic-parallelism child grid
 //     (sssp_process_buffer, :82-104, or unorder_blockQueue_kernel, :57-78) per buffer.
-// Here the buffers are consumed in-kernel by the warp, the CTA or every CTA of
+// Here the buffers are consumed in-kernel by the warp, the CTA or every warp of
 // the team, and the frontier is a device queue filled by warp-aggregated
 // appends, deduplicated with per-vertex stamps.
 //
@@ -24,12 +24,26 @@
 // gives the reference's unordered frontier order.  Any delta yields the same
 // exact distances; it only changes the work and the number of iterations.
 //
+// Work distribution.  Inside an iteration every warp pulls its own work items
+// from 8 striped atomic counters (no CTA-wide synchronisation on the hot path):
+//   heavy items   128 16-byte chunks (512 edges) of the flat chunk space of the
+//                 grid-tier list H that the previous iteration collected;
+//   vertex items  32 frontier vertices, one per lane.
+// A vertex of out-degree d is handled by tier:
+//   d < threshold                     small: warp-flat loop over the warp's small rows
+//   WARP  level, or HYBRID d < block  warp tier: the warp walks the row, 128 edges a step
+//   BLOCK level, or HYBRID d < grid   block tier: appended to the CTA list in shared
+//                                     memory, walked by all of the CTA's warps once per
+//                                     iteration (the warp tier takes it if the list is full)
+//   GRID  level, or HYBRID d >= grid  grid tier: appended to H, walked next iteration by
+//                                     every warp of the team
+//
 // Iteration protocol (per team of co-resident CTAs, one barrier per iteration):
 //   iteration it consumes either the near queue Q[it&1] or, on a bucket advance,
-//   the far pile of the previous epoch, plus the grid-tier list H[(it-1)%3] that
-//   the previous iteration collected.  It appends to Q[(it+1)&1], to the far pile
-//   of the current epoch and to H[it%3].  All counters live in 3-slot rings so a
-//   slot is reset at least one barrier before it is reused.
+//   the far pile of the previous epoch, plus H of iteration it-1.  It appends to
+//   Q[(it+1)&1], to the far pile of the current epoch and to H of iteration it.
+//   All counters live in 3-slot rings so a slot is reset at least one barrier
+//   before it is reused.
 #pragma once
 
 #include <cstdint>
@@ -42,18 +56,21 @@ constexpr uint32_t kFull = 0xffffffffu;
 constexpr uint32_t kInf = NPS_INF;
 constexpr int kHeavyShift = 36;  // heavy counter packs (count << 36) | chunk_offset
 constexpr unsigned long long kHeavyMask = (1ull << kHeavyShift) - 1;
+constexpr int kStripes = 8;            // striped work counters
+constexpr int kHeavyItemChunks = 128;  // chunks (4 edges each) per heavy work item
+constexpr int kBlockListCap = 512;     // CTA list entries (block tier)
 
 // Per-instance device counters.  Zeroed by the host before a launch.
 struct __align__(128) Counters {
   uint32_t qtail[3];   // near-queue tails, slot = iteration % 3
   uint32_t ftail[3];   // far-pile tails,   slot = epoch % 3
-  uint32_t work[3];    // dynamic work-item counters, slot = iteration % 3
   uint32_t fmin[3];    // min distance pushed into the far pile on an advance, slot = epoch % 3
-  unsigned long long heavy[3];  // grid-tier list counter, slot = iteration % 3
   uint32_t status;     // NPS_OK or the first error
+  unsigned long long heavy[3];  // grid-tier list counter, slot = iteration % 3
   uint32_t iterations;
   uint32_t buckets;
   uint32_t reached;    // vertices whose distance left INF during the run
+  uint32_t pad0;
   unsigned long long edges;
   unsigned long long improvements;
   unsigned long long processed;
@@ -62,7 +79,9 @@ struct __align__(128) Counters {
   unsigned long long it_edges[3];
   unsigned long long it_impr[3];
   uint32_t it_reached[3];
-  uint32_t pad[5];
+  uint32_t pad1[3];
+  // striped work counters, one 128-byte line each: work[slot][stripe * 32]
+  uint32_t work[3][kStripes * 32];
 };
 
 struct InstDesc {
@@ -88,7 +107,7 @@ struct InstDesc {
   uint32_t trace_cap;
   uint32_t delta;
   int32_t level;
-  int32_t t1, t2, t3;   // tier thresholds: [t1,t2) warp, [t2,t3) block, >= t3 grid; < t1 small
+  int32_t t1, t2, t3;   // threshold, block_threshold, grid_threshold
   int32_t policy;
   int32_t vec_ok;       // col / w are 16-byte aligned
   int32_t pad0;
@@ -117,7 +136,8 @@ struct LaunchParams {
   const TeamDesc* teams;
   int32_t n_teams;
   int32_t fault_inject_wait;  // 1: the first barrier waits for an arrival that never comes
-  uint32_t* bar;              // per-team barrier counters, 32 words apart
+  uint32_t* bar;              // per-team barrier words (see team_barrier), bar_stride words per team
+  uint32_t bar_stride;
   uint32_t* abort_flag;
   unsigned long long timeout_ns;     // bound on each wait
   unsigned long long run_budget_ns;  // bound on the whole launch
@@ -178,6 +198,26 @@ __device__ __forceinline__ int deg_bin(int32_t d) {
   return b > 7 ? 7 : b;
 }
 
+// Distance read for the pre-check `nd < dist[v]` before atomicMin.  With
+// NPS_DIST_L1 the read may hit a line cached in L1 earlier in the iteration:
+// such a value can only be higher than the current one (distances only drop),
+// so a stale hit costs an atomicMin that does not improve, never a lost update.
+__device__ __forceinline__ uint32_t ld_dist(const uint32_t* p) {
+#ifdef NPS_DIST_L1
+  return __ldca(p);
+#else
+  return __ldcg(p);
+#endif
+}
+
+__device__ __forceinline__ uint32_t tent(uint32_t du, uint32_t w) {
+  return (w >= kInf || du >= kInf) ? kInf : du + w;  // both < 2^30, so no wrap
+}
+
+__device__ __forceinline__ uint32_t row_chunks(int32_t s, int32_t e) {
+  return (uint32_t)(((e - 1) >> 2) - (s >> 2) + 1);
+}
+
 // ---------------------------------------------------------------------------
 // Per-iteration context, identical in every CTA of a team.
 struct IterCtx {
@@ -192,7 +232,9 @@ struct IterCtx {
   int4* heavy;       // grid-tier list receiving appends
   unsigned long long* heavy_ctr;
   uint32_t hcap;     // capacity of that list
-  int32_t t1, t2, t3;
+  int32_t t_warp;    // degree >= t_warp leaves the small path
+  int32_t t_block;   // degree >= t_block goes to the CTA list
+  int32_t t_grid;    // degree >= t_grid goes to H
 };
 
 // Thread-local accumulators, reduced per CTA.
@@ -203,107 +245,189 @@ struct Acc {
   uint32_t processed;
 };
 
-// Relax one candidate edge u->v with tentative distance nd.  Returns which
-// queue (if any) v must be appended to.  Exact: atomicMin decides.
-__device__ __forceinline__ void relax_one(const InstDesc& I, const IterCtx& C, bool valid, int32_t v,
-                                          uint32_t nd, bool& pn, bool& pf, Acc& acc) {
-  pn = false;
-  pf = false;
-  if (!valid) return;
-  acc.edges++;
-  if ((uint32_t)v >= (uint32_t)I.n) {  // neighbour id outside [0, n): record and skip
-    atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_FORMAT);
-    return;
+// ---------------------------------------------------------------------------
+// Batched relaxation: K candidate edges per lane.  All K distance loads are
+// issued before any is used and all K atomicMin before any result is used, so
+// one lane keeps K independent L2 requests in flight.  Returns, per candidate,
+// whether the head must be appended to the near queue (pn) or far pile (pf).
+template <int K>
+__device__ __forceinline__ void relax_batch(const InstDesc& I, const IterCtx& C, const bool (&valid)[K],
+                                            const int32_t (&v)[K], const uint32_t (&nd)[K], bool (&pn)[K],
+                                            bool (&pf)[K], Acc& acc) {
+  uint32_t cur[K];
+  bool go[K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    go[j] = valid[j];
+    if (valid[j]) {
+      acc.edges++;
+      if ((uint32_t)v[j] >= (uint32_t)I.n) {  // neighbour id outside [0, n): record and skip
+        atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_FORMAT);
+        go[j] = false;
+      } else if (nd[j] >= kInf) {
+        go[j] = false;
+      }
+    }
   }
-  if (nd >= kInf) return;
-  uint32_t cur = __ldcg(I.dist + v);
-  if (nd >= cur) return;
-  uint32_t old = atomicMin(I.dist + v, nd);
-  if (nd >= old) return;
-  acc.impr++;
-  if (old == kInf) acc.reached++;
-  if (nd < C.T) {
-    if (__ldcg(I.mark + v) != C.snear) pn = atomicExch(I.mark + v, C.snear) != C.snear;
-  } else {
-    if (__ldcg(I.fmark + v) != C.sfar) {
-      pf = atomicExch(I.fmark + v, C.sfar) != C.sfar;
-      if (pf && C.fp_min) atomicMin(C.fp_min, nd);
+#pragma unroll
+  for (int j = 0; j < K; ++j) cur[j] = go[j] ? ld_dist(I.dist + v[j]) : 0u;
+  uint32_t old[K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    go[j] = go[j] && nd[j] < cur[j];
+    old[j] = go[j] ? atomicMin(I.dist + v[j], nd[j]) : 0u;
+  }
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    pn[j] = false;
+    pf[j] = false;
+    if (go[j] && nd[j] < old[j]) {
+      acc.impr++;
+      if (old[j] == kInf) acc.reached++;
+      if (nd[j] < C.T) {
+        if (__ldcg(I.mark + v[j]) != C.snear) pn[j] = atomicExch(I.mark + v[j], C.snear) != C.snear;
+      } else {
+        if (__ldcg(I.fmark + v[j]) != C.sfar) {
+          pf[j] = atomicExch(I.fmark + v[j], C.sfar) != C.sfar;
+          if (pf[j] && C.fp_min) atomicMin(C.fp_min, nd[j]);
+        }
+      }
     }
   }
 }
 
-__device__ __forceinline__ uint32_t tent(uint32_t du, uint32_t w) {
-  return (w >= kInf || du >= kInf) ? kInf : du + w;  // both < 2^30, so no wrap
-}
-
-// Warp-aggregated append of one item per lane.
-__device__ __forceinline__ void append1(int32_t* q, uint32_t* tail, uint32_t cap, bool f, int32_t v,
-                                        uint32_t* status, int lane) {
-  uint32_t b = __ballot_sync(kFull, f);
-  if (b == 0) return;
-  uint32_t base = 0;
-  int leader = __ffs(b) - 1;
-  if (lane == leader) base = atomicAdd(tail, (uint32_t)__popc(b));
-  base = __shfl_sync(kFull, base, leader);
-  uint32_t pos = base + __popc(b & lanemask_lt());
-  if (f) {
-    if (pos < cap) q[pos] = v;
-    else atomicCAS(status, 0u, (uint32_t)NPS_ERR_CAPACITY);
+// Warp-aggregated append of up to K items per lane: one ballot per slot, one
+// atomicAdd per warp.  Warp-collective.
+template <int K>
+__device__ __forceinline__ void append_k(int32_t* q, uint32_t* tail, uint32_t cap, const bool (&f)[K],
+                                         const int32_t (&v)[K], uint32_t* status, int lane) {
+  uint32_t b[K];
+  uint32_t tot = 0;
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    b[j] = __ballot_sync(kFull, f[j]);
+    tot += __popc(b[j]);
   }
-}
-
-// Warp-aggregated append of up to four items per lane (one ballot per slot).
-__device__ __forceinline__ void append4(int32_t* q, uint32_t* tail, uint32_t cap, bool f0, bool f1,
-                                        bool f2, bool f3, int32_t v0, int32_t v1, int32_t v2,
-                                        int32_t v3, uint32_t* status, int lane) {
-  uint32_t b0 = __ballot_sync(kFull, f0), b1 = __ballot_sync(kFull, f1);
-  uint32_t b2 = __ballot_sync(kFull, f2), b3 = __ballot_sync(kFull, f3);
-  uint32_t tot = __popc(b0) + __popc(b1) + __popc(b2) + __popc(b3);
   if (tot == 0) return;
   uint32_t base = 0;
   if (lane == 0) base = atomicAdd(tail, tot);
   base = __shfl_sync(kFull, base, 0);
-  uint32_t lt = lanemask_lt();
-  uint32_t o = base;
+  const uint32_t lt = lanemask_lt();
   bool over = false;
-  if (f0) { uint32_t p = o + __popc(b0 & lt); if (p < cap) q[p] = v0; else over = true; }
-  o += __popc(b0);
-  if (f1) { uint32_t p = o + __popc(b1 & lt); if (p < cap) q[p] = v1; else over = true; }
-  o += __popc(b1);
-  if (f2) { uint32_t p = o + __popc(b2 & lt); if (p < cap) q[p] = v2; else over = true; }
-  o += __popc(b2);
-  if (f3) { uint32_t p = o + __popc(b3 & lt); if (p < cap) q[p] = v3; else over = true; }
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    if (f[j]) {
+      const uint32_t p = base + __popc(b[j] & lt);
+      if (p < cap) q[p] = v[j];
+      else over = true;
+    }
+    base += __popc(b[j]);
+  }
   if (over) atomicCAS(status, 0u, (uint32_t)NPS_ERR_CAPACITY);
 }
 
-// Relax the (up to) four edges of the 16-byte chunk starting at edge index c
-// that fall inside [s, e).  Loads the column and weight chunks with one int4
-// load each when aligned and in bounds.  Warp-collective (ballots inside).
-__device__ __forceinline__ void relax_chunk(const InstDesc& I, const IterCtx& C, bool act, int32_t c,
-                                            int32_t s, int32_t e, uint32_t du, Acc& acc, int lane) {
-  int4 cv = make_int4(0, 0, 0, 0), wv = make_int4(0, 0, 0, 0);
-  if (act) {
-    if (I.vec_ok && c + 4 <= I.m) {
-      cv = ld_stream_v4(I.col + c);
-      wv = ld_stream_v4((const int32_t*)I.w + c);
-    } else {
-      if (c >= s && c < e) { cv.x = ld_stream(I.col + c); wv.x = ld_stream((const int32_t*)I.w + c); }
-      if (c + 1 >= s && c + 1 < e) { cv.y = ld_stream(I.col + c + 1); wv.y = ld_stream((const int32_t*)I.w + c + 1); }
-      if (c + 2 >= s && c + 2 < e) { cv.z = ld_stream(I.col + c + 2); wv.z = ld_stream((const int32_t*)I.w + c + 2); }
-      if (c + 3 >= s && c + 3 < e) { cv.w = ld_stream(I.col + c + 3); wv.w = ld_stream((const int32_t*)I.w + c + 3); }
-    }
+// Per-warp staging of queue appends in shared memory.  A warp collects the
+// vertices it pushes and moves them to the global queue 32 at a time (one
+// atomicAdd on the queue tail per >= 32 entries, one coalesced 128-byte store
+// per 32), so warps do not serialise on the tail counter every round.
+constexpr int kStage = 192;  // >= 31 left over + 4 * 32 from one append
+
+struct Stage {
+  int32_t* nbuf;   // near-queue staging (kStage entries, shared memory)
+  int32_t* fbuf;   // far-pile staging
+  uint32_t ncnt;   // warp-uniform fill counts
+  uint32_t fcnt;
+};
+
+// Move the first `nflush` staged entries to q and shift the rest down.
+__device__ __forceinline__ void stage_flush(int32_t* buf, uint32_t& cnt, uint32_t nflush, int32_t* q,
+                                            uint32_t* tail, uint32_t cap, uint32_t* status, int lane) {
+  __syncwarp();
+  uint32_t base = 0;
+  if (lane == 0) base = atomicAdd(tail, nflush);
+  base = __shfl_sync(kFull, base, 0);
+  for (uint32_t i = lane; i < nflush; i += 32) {
+    if (base + i < cap) q[base + i] = buf[i];
+    else atomicCAS(status, 0u, (uint32_t)NPS_ERR_CAPACITY);
   }
-  bool n0, n1, n2, n3, f0, f1, f2, f3;
-  relax_one(I, C, act && c >= s && c < e, cv.x, tent(du, (uint32_t)wv.x), n0, f0, acc);
-  relax_one(I, C, act && c + 1 >= s && c + 1 < e, cv.y, tent(du, (uint32_t)wv.y), n1, f1, acc);
-  relax_one(I, C, act && c + 2 >= s && c + 2 < e, cv.z, tent(du, (uint32_t)wv.z), n2, f2, acc);
-  relax_one(I, C, act && c + 3 >= s && c + 3 < e, cv.w, tent(du, (uint32_t)wv.w), n3, f3, acc);
-  append4(C.qn, C.qn_tail, I.qcap, n0, n1, n2, n3, cv.x, cv.y, cv.z, cv.w, &I.ctr->status, lane);
-  append4(C.fp, C.fp_tail, I.qcap, f0, f1, f2, f3, cv.x, cv.y, cv.z, cv.w, &I.ctr->status, lane);
+  const uint32_t rem = cnt - nflush;
+  int32_t t = 0;
+  if ((uint32_t)lane < rem) t = buf[nflush + lane];
+  __syncwarp();
+  if ((uint32_t)lane < rem) buf[lane] = t;
+  __syncwarp();
+  cnt = rem;
 }
 
-__device__ __forceinline__ uint32_t row_chunks(int32_t s, int32_t e) {
-  return (uint32_t)(((e - 1) >> 2) - (s >> 2) + 1);
+template <int K>
+__device__ __forceinline__ void stage_k(int32_t* buf, uint32_t& cnt, const bool (&f)[K], const int32_t (&v)[K],
+                                        int32_t* q, uint32_t* tail, uint32_t cap, uint32_t* status, int lane) {
+  uint32_t b[K];
+  uint32_t tot = 0;
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    b[j] = __ballot_sync(kFull, f[j]);
+    tot += __popc(b[j]);
+  }
+  if (tot == 0) return;
+  const uint32_t lt = lanemask_lt();
+  uint32_t base = cnt;
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    if (f[j]) buf[base + __popc(b[j] & lt)] = v[j];
+    base += __popc(b[j]);
+  }
+  cnt += tot;
+  if (cnt >= 32) stage_flush(buf, cnt, cnt & ~31u, q, tail, cap, status, lane);
+}
+
+// End of an iteration: everything staged goes to the global queues.
+__device__ __forceinline__ void stage_drain(Stage& S, const IterCtx& C, uint32_t qcap, uint32_t* status, int lane) {
+  if (S.ncnt) stage_flush(S.nbuf, S.ncnt, S.ncnt, C.qn, C.qn_tail, qcap, status, lane);
+  if (S.fcnt) stage_flush(S.fbuf, S.fcnt, S.fcnt, C.fp, C.fp_tail, qcap, status, lane);
+}
+
+template <int K>
+__device__ __forceinline__ void relax_and_push(const InstDesc& I, const IterCtx& C, const bool (&valid)[K],
+                                               const int32_t (&v)[K], const uint32_t (&nd)[K], Acc& acc,
+                                               Stage& S, int lane) {
+  bool pn[K], pf[K];
+  relax_batch<K>(I, C, valid, v, nd, pn, pf, acc);
+  stage_k<K>(S.nbuf, S.ncnt, pn, v, C.qn, C.qn_tail, I.qcap, &I.ctr->status, lane);
+  stage_k<K>(S.fbuf, S.fcnt, pf, v, C.fp, C.fp_tail, I.qcap, &I.ctr->status, lane);
+}
+
+// Load the 16-byte chunk at edge index c (4-aligned) of the column and weight
+// arrays: one int4 load each when aligned and in bounds, else element-wise
+// loads of the positions inside [s, e).
+__device__ __forceinline__ void load_chunk(const InstDesc& I, bool act, int32_t c, int32_t s, int32_t e,
+                                           int4& cv, int4& wv) {
+  cv = make_int4(0, 0, 0, 0);
+  wv = make_int4(0, 0, 0, 0);
+  if (!act) return;
+  if (I.vec_ok && c + 4 <= I.m) {
+    cv = ld_stream_v4(I.col + c);
+    wv = ld_stream_v4((const int32_t*)I.w + c);
+  } else {
+    const int32_t* wp = (const int32_t*)I.w;
+    if (c >= s && c < e) { cv.x = ld_stream(I.col + c); wv.x = ld_stream(wp + c); }
+    if (c + 1 >= s && c + 1 < e) { cv.y = ld_stream(I.col + c + 1); wv.y = ld_stream(wp + c + 1); }
+    if (c + 2 >= s && c + 2 < e) { cv.z = ld_stream(I.col + c + 2); wv.z = ld_stream(wp + c + 2); }
+    if (c + 3 >= s && c + 3 < e) { cv.w = ld_stream(I.col + c + 3); wv.w = ld_stream(wp + c + 3); }
+  }
+}
+
+// Relax the edges of chunk c that fall inside [s, e).  Warp-collective.
+__device__ __forceinline__ void relax_chunk(const InstDesc& I, const IterCtx& C, bool act, int32_t c,
+                                            int32_t s, int32_t e, uint32_t du, Acc& acc, Stage& S, int lane) {
+  int4 cv, wv;
+  load_chunk(I, act, c, s, e, cv, wv);
+  const bool valid[4] = {act && c >= s && c < e, act && c + 1 >= s && c + 1 < e,
+                         act && c + 2 >= s && c + 2 < e, act && c + 3 >= s && c + 3 < e};
+  const int32_t v[4] = {cv.x, cv.y, cv.z, cv.w};
+  const uint32_t nd[4] = {tent(du, (uint32_t)wv.x), tent(du, (uint32_t)wv.y), tent(du, (uint32_t)wv.z),
+                          tent(du, (uint32_t)wv.w)};
+  relax_and_push<4>(I, C, valid, v, nd, acc, S, lane);
 }
 
 // ---------------------------------------------------------------------------
@@ -311,23 +435,33 @@ __device__ __forceinline__ uint32_t row_chunks(int32_t s, int32_t e) {
 
 template <int BS>
 struct Smem {
-  unsigned long long blk_ctr;  // (count << 32) | chunk offset
-  uint32_t item;
+  unsigned long long blk_ctr;  // CTA list (block tier): (entries << 32) | chunks, one atomic
   int32_t ok;
   uint32_t hist[8];
-  int4 blk[BS];                // block-tier entries {s, e, du, chunk offset}
+  int4 blk[kBlockListCap];     // block-tier entries {s, e, vertex, chunk offset}
+  int32_t stage[BS / 32][2][kStage];  // per-warp append staging: [near, far]
   uint32_t red[4][BS / 32];
   float feat[NPS_MLP_IN];
   float hid[NPS_MLP_HID];
   int32_t pol_choice[2];
   TeamDesc team;
   int32_t team_id;
+  uint32_t rank;
+  uint32_t bc_q, bc_f, bc_m;   // counters broadcast after a barrier
+  unsigned long long bc_h;
   unsigned long long t_start;
 };
 
 // Team barrier over the CTAs of one team.  Bounded: gives up after timeout_ns
 // (setting NPS_ERR_TIMEOUT and the abort flag) or when the abort flag is set.
 // Returns false when the computation must stop.
+//
+// Two-level arrival: the CTAs of each group of kBarGroup count in on their
+// group's word; the last of a group counts the group in on the root word; the
+// last group publishes the new generation, which every CTA polls.  Words are
+// 128 bytes apart: bar[0] root, bar[32] generation, bar[64 + 32 g] group g.
+constexpr uint32_t kBarGroup = 16;
+
 template <int BS>
 __device__ __forceinline__ bool team_barrier(const LaunchParams& P, Smem<BS>& sm, uint32_t* bar,
                                              uint32_t& epoch, uint32_t team_size,
@@ -339,13 +473,23 @@ __device__ __forceinline__ bool team_barrier(const LaunchParams& P, Smem<BS>& sm
       atomicExch(P.abort_flag, 1u);
     }
     epoch += 1;
-    uint32_t target = epoch * team_size + (inject ? 1u : 0u);
+    const uint32_t rank = sm.rank;
+    const uint32_t g = rank / kBarGroup;
+    const uint32_t gsz = min(kBarGroup, team_size - g * kBarGroup);
+    const uint32_t ngroups = (team_size + kBarGroup - 1) / kBarGroup;
     __threadfence();
-    atomicAdd(bar, 1u);
+    if (atomicAdd(bar + 64 + 32 * g, 1u) == epoch * gsz - 1) {
+      __threadfence();
+      if (atomicAdd(bar, 1u) == epoch * ngroups - 1) {
+        __threadfence();
+        atomicExch(bar + 32, epoch);
+      }
+    }
+    const uint32_t target = epoch + (inject ? 1u : 0u);
     unsigned long long t0 = globaltimer_ns();
     int ok = 1;
     uint32_t spins = 0;
-    while ((int32_t)(ld_acquire_u32(bar) - target) < 0) {
+    while ((int32_t)(ld_acquire_u32(bar + 32) - target) < 0) {
       if (ld_relaxed_u32(P.abort_flag)) { ok = 0; break; }
       if ((++spins & 15u) == 0 && globaltimer_ns() - t0 > P.timeout_ns) {
         atomicCAS(status, 0u, (uint32_t)NPS_ERR_TIMEOUT);
@@ -396,20 +540,22 @@ __device__ __forceinline__ void block_sum4(Smem<BS>& sm, uint32_t a, uint32_t b,
 }
 
 // ---------------------------------------------------------------------------
-// Process one frontier chunk of BS vertices (or far-pile entries on a bucket
-// advance).  Degree tiers:
-//   deg <  t1       : warp-flat loop (warp scan of degrees, one edge per lane)
-//   [t1, t2)        : warp tier  -- the owning warp walks the row with int4 chunks
-//   [t2, t3)        : block tier -- appended to the CTA list, walked by all warps
-//   >= t3           : grid tier  -- appended to H, walked by every CTA next iteration
+// Walk one row [s, e) with the whole warp, 128 edges (one int4 per lane) a step.
+__device__ __forceinline__ void warp_row(const InstDesc& I, const IterCtx& C, int32_t s, int32_t e, uint32_t du,
+                                         Acc& acc, Stage& S, int lane) {
+  for (int32_t c0 = s & ~3; c0 < e; c0 += 128) {
+    const int32_t c = c0 + lane * 4;
+    relax_chunk(I, C, c < e, c, s, e, du, acc, S, lane);
+  }
+}
+
+// Vertex work item: 32 frontier entries (or far-pile entries on a bucket
+// advance), one per lane.  Warp-collective.
 template <int BS>
-__device__ __forceinline__ void process_vertices(const InstDesc& I, const IterCtx& C, Smem<BS>& sm,
-                                                 const int32_t* src_q, uint32_t idx_base,
-                                                 uint32_t src_len, bool advance, uint32_t T_old,
-                                                 bool want_hist, Acc& acc) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int NW = BS / 32;
-  uint32_t idx = idx_base + threadIdx.x;
+__device__ __forceinline__ void process_vertex_item(const InstDesc& I, const IterCtx& C, Smem<BS>& sm,
+                                                    const int32_t* src_q, uint32_t idx, uint32_t src_len,
+                                                    bool advance, uint32_t T_old, bool want_hist, Acc& acc,
+                                                    Stage& S, int lane) {
   int32_t v = -1, s = 0, e = 0;
   uint32_t du = 0;
   bool repush = false;
@@ -441,63 +587,75 @@ __device__ __forceinline__ void process_vertices(const InstDesc& I, const IterCt
       if (want_hist) atomicAdd(&sm.hist[deg_bin(e - s)], 1u);
     }
   }
-  if (advance) append1(C.fp, C.fp_tail, I.qcap, repush, rv, &I.ctr->status, lane);
+  if (advance) {
+    const bool f[1] = {repush};
+    const int32_t vv[1] = {rv};
+    stage_k<1>(S.fbuf, S.fcnt, f, vv, C.fp, C.fp_tail, I.qcap, &I.ctr->status, lane);
+  }
   const int32_t deg = e - s;
-  const bool small = deg > 0 && deg < C.t1;
-  const bool wtier = deg >= C.t1 && deg < C.t2 && deg > 0;
-  const bool btier = deg >= C.t2 && deg < C.t3 && deg > 0;
-  const bool gtier = deg >= C.t3 && deg > 0;
+  const bool small = deg > 0 && deg < C.t_warp;
+  bool wtier = deg >= C.t_warp && deg < C.t_block;
+  const bool btier = deg >= C.t_block && deg < C.t_grid;
+  const bool gtier = deg >= C.t_grid && deg > 0;
   if (btier) {
-    uint32_t nch = row_chunks(s, e);
-    unsigned long long old = atomicAdd(&sm.blk_ctr, (1ull << 32) | nch);
-    sm.blk[old >> 32] = make_int4(s, e, (int32_t)du, (int32_t)(uint32_t)old);
+    // slot and chunk offset from one atomic, so offsets increase with the slot
+    const unsigned long long old = atomicAdd(&sm.blk_ctr, (1ull << 32) | row_chunks(s, e));
+    const uint32_t slot = (uint32_t)(old >> 32);
+    if (slot < (uint32_t)kBlockListCap) sm.blk[slot] = make_int4(s, e, v, (int32_t)(uint32_t)old);
+    else wtier = true;  // CTA list full: the warp walks the row itself
   }
   if (gtier) {
-    uint32_t nch = row_chunks(s, e);
-    unsigned long long old = atomicAdd(C.heavy_ctr, (1ull << kHeavyShift) | nch);
-    uint32_t slot = (uint32_t)(old >> kHeavyShift);
+    const uint32_t nch = row_chunks(s, e);
+    const unsigned long long old = atomicAdd(C.heavy_ctr, (1ull << kHeavyShift) | nch);
+    const uint32_t slot = (uint32_t)(old >> kHeavyShift);
     if (slot < C.hcap) C.heavy[slot] = make_int4(s, e, v, (int32_t)(uint32_t)(old & kHeavyMask));
     else atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_CAPACITY);
   }
 
-  // ---- small vertices: warp-flat edge loop
+  // ---- small rows: warp-flat loop, four edges per lane per round
   {
-    uint32_t d = small ? (uint32_t)deg : 0u;
+    const uint32_t d = small ? (uint32_t)deg : 0u;
     uint32_t incl = d;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      uint32_t t = __shfl_up_sync(kFull, incl, o);
+      const uint32_t t = __shfl_up_sync(kFull, incl, o);
       if (lane >= o) incl += t;
     }
     const uint32_t total = __shfl_sync(kFull, incl, 31);
     const uint32_t excl = incl - d;
-    for (uint32_t k0 = 0; k0 < total; k0 += 32) {
-      const uint32_t k = k0 + lane;
-      const bool valid = k < total;
-      int j = 0;
+    for (uint32_t k0 = 0; k0 < total; k0 += 128) {
+      bool valid[4];
+      int32_t ei[4];
+      uint32_t dj[4];
 #pragma unroll
-      for (int step = 16; step >= 1; step >>= 1) {
-        uint32_t x = __shfl_sync(kFull, excl, j + step);
-        if (x <= k) j += step;
+      for (int j = 0; j < 4; ++j) {
+        const uint32_t k = k0 + j * 32 + lane;
+        valid[j] = k < total;
+        int o = 0;
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1) {
+          const uint32_t x = __shfl_sync(kFull, excl, o + step);
+          if (x <= k) o += step;
+        }
+        const int32_t so = __shfl_sync(kFull, s, o);
+        const uint32_t eo = __shfl_sync(kFull, excl, o);
+        dj[j] = __shfl_sync(kFull, du, o);
+        ei[j] = so + (int32_t)(k - eo);
       }
-      const int32_t sj = __shfl_sync(kFull, s, j);
-      const uint32_t duj = __shfl_sync(kFull, du, j);
-      const uint32_t exj = __shfl_sync(kFull, excl, j);
-      int32_t nb = 0;
-      uint32_t wt = 0;
-      if (valid) {
-        int32_t ei = sj + (int32_t)(k - exj);
-        nb = ld_stream(I.col + ei);
-        wt = (uint32_t)ld_stream((const int32_t*)I.w + ei);
+      int32_t nb[4];
+      uint32_t nd[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        nb[j] = valid[j] ? ld_stream(I.col + ei[j]) : 0;
+        nd[j] = valid[j] ? (uint32_t)ld_stream((const int32_t*)I.w + ei[j]) : 0u;
       }
-      bool pn, pf;
-      relax_one(I, C, valid, nb, tent(duj, wt), pn, pf, acc);
-      append1(C.qn, C.qn_tail, I.qcap, pn, nb, &I.ctr->status, lane);
-      append1(C.fp, C.fp_tail, I.qcap, pf, nb, &I.ctr->status, lane);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) nd[j] = tent(dj[j], nd[j]);
+      relax_and_push<4>(I, C, valid, nb, nd, acc, S, lane);
     }
   }
 
-  // ---- warp tier: the warp walks each of its rows, 128 edges per step
+  // ---- warp tier: the warp walks each of its rows
   {
     uint32_t wb = __ballot_sync(kFull, wtier);
     while (wb) {
@@ -506,52 +664,48 @@ __device__ __forceinline__ void process_vertices(const InstDesc& I, const IterCt
       const int32_t rs = __shfl_sync(kFull, s, src_lane);
       const int32_t re = __shfl_sync(kFull, e, src_lane);
       const uint32_t rdu = __shfl_sync(kFull, du, src_lane);
-      for (int32_t c0 = rs & ~3; c0 < re; c0 += 128) {
-        const int32_t c = c0 + lane * 4;
-        relax_chunk(I, C, c < re, c, rs, re, rdu, acc, lane);
-      }
+      warp_row(I, C, rs, re, rdu, acc, S, lane);
     }
-  }
-
-  // ---- block tier: every warp of the CTA walks the flat chunk space of the list
-  __syncthreads();
-  const unsigned long long bc = sm.blk_ctr;
-  const uint32_t bcnt = (uint32_t)(bc >> 32), btot = (uint32_t)bc;
-  for (uint32_t k0 = warp * 32; k0 < btot; k0 += NW * 32) {
-    const uint32_t k = k0 + lane;
-    const bool act = k < btot;
-    int lo = 0, hi = (int)bcnt - 1;
-    while (lo < hi) {
-      int mid = (lo + hi + 1) >> 1;
-      if ((uint32_t)sm.blk[mid].w <= k) lo = mid;
-      else hi = mid - 1;
-    }
-    const int4 ent = sm.blk[lo];
-    const int32_t c = (ent.x & ~3) + 4 * (int32_t)(k - (uint32_t)ent.w);
-    relax_chunk(I, C, act, c, ent.x, ent.y, (uint32_t)ent.z, acc, lane);
   }
 }
 
-// Grid-tier work item: BS chunks of the flat chunk space of list H.
-template <int BS>
-__device__ __forceinline__ void process_heavy(const InstDesc& I, const IterCtx& C, const int4* H,
-                                              uint32_t hcnt, unsigned long long htot,
-                                              unsigned long long k_base, Acc& acc) {
-  const int lane = threadIdx.x & 31;
-  const unsigned long long k = k_base + threadIdx.x;
-  const bool act = k < htot;
-  // largest j with offset(j) <= k
-  int lo = 0, hi = (int)hcnt - 1;
+// Flat chunk-space walk of a list of rows {s, e, vertex, chunk offset} sorted by
+// offset: chunks [k_begin, k_end) are handled by this warp, each lane takes
+// every 32nd chunk.  Distances of the row owners are re-read here (the list may
+// have been built an iteration earlier).  Warp-collective.
+__device__ __forceinline__ void walk_chunks(const InstDesc& I, const IterCtx& C, const int4* L, uint32_t cnt,
+                                            unsigned long long k_begin, unsigned long long k_end, Acc& acc,
+                                            Stage& S, int lane) {
+  if (k_begin >= k_end || cnt == 0) return;
+  // owner of the lane's first chunk: largest j with offset(j) <= k
+  unsigned long long k = k_begin + lane;
+  int lo = 0, hi = (int)cnt - 1;
   while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    int4 em = H[mid];
-    if ((unsigned long long)(uint32_t)em.w <= k) lo = mid;
+    const int mid = (lo + hi + 1) >> 1;
+    if ((unsigned long long)(uint32_t)L[mid].w <= k) lo = mid;
     else hi = mid - 1;
   }
-  int4 ent = H[lo];
-  uint32_t du = act ? __ldcg(I.dist + ent.z) : 0u;
-  const int32_t c = (ent.x & ~3) + 4 * (int32_t)(k - (uint32_t)ent.w);
-  relax_chunk(I, C, act, c, ent.x, ent.y, du, acc, lane);
+  int j = lo;
+  int4 ent = L[j];
+  uint32_t nxt = (j + 1 < (int)cnt) ? (uint32_t)L[j + 1].w : 0xffffffffu;
+  // the owner's distance is read when the owner changes; a value that has
+  // dropped since only makes this walk relax with a larger tentative distance,
+  // and the owner is back in a queue for every drop
+  uint32_t du = (k < k_end) ? __ldcg(I.dist + ent.z) : 0u;
+  for (unsigned long long k0 = k_begin; k0 < k_end; k0 += 32) {
+    k = k0 + lane;
+    const bool act = k < k_end;
+    bool moved = false;
+    while (act && j + 1 < (int)cnt && (unsigned long long)nxt <= k) {
+      ++j;
+      ent = L[j];
+      nxt = (j + 1 < (int)cnt) ? (uint32_t)L[j + 1].w : 0xffffffffu;
+      moved = true;
+    }
+    if (moved) du = __ldcg(I.dist + ent.z);
+    const int32_t c = (ent.x & ~3) + 4 * (int32_t)(k - (uint32_t)ent.w);
+    relax_chunk(I, C, act, c, ent.x, ent.y, du, acc, S, lane);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -574,48 +728,48 @@ __device__ __forceinline__ void policy_eval(const PolicyDev* pol, Smem<BS>& sm) 
   }
   __syncthreads();
   if (t == 0) {
-    float best = -3.0e38f;
-    int bd = 0;
     float lg[NPS_MLP_OUT];
     for (int o = 0; o < NPS_MLP_OUT; ++o) {
       float a = pol->b2[o];
       for (int h = 0; h < NPS_MLP_HID; ++h) a = fmaf(bf16_bits_to_float(pol->w2[o * NPS_MLP_HID + h]), sm.hid[h], a);
       lg[o] = a;
     }
-    for (int o = 0; o < 11; ++o)
-      if (lg[o] > best) { best = lg[o]; bd = o; }
+    int bd = 0;
+    for (int o = 1; o < 11; ++o)
+      if (lg[o] > lg[bd]) bd = o;
     int bl = 0;
-    best = lg[11];
     for (int o = 1; o < 3; ++o)
-      if (lg[11 + o] > best) { best = lg[11 + o]; bl = o; }
+      if (lg[11 + o] > lg[11 + bl]) bl = o;
     sm.pol_choice[0] = bd;
     sm.pol_choice[1] = bl;
   }
   __syncthreads();
 }
 
-// Thresholds (t1, t2, t3) for a consolidation level.
+// Tier thresholds (warp, block, grid) for a consolidation level.
 __device__ __forceinline__ void level_thresholds(int level, int32_t thr, int32_t bthr, int32_t gthr,
-                                                 int32_t& t1, int32_t& t2, int32_t& t3) {
+                                                 int32_t& tw, int32_t& tb, int32_t& tg) {
   const int32_t big = 0x7fffffff;
   switch (level) {
-    case NPS_LEVEL_WARP: t1 = thr; t2 = big; t3 = big; break;
-    case NPS_LEVEL_GRID: t1 = thr; t2 = thr; t3 = thr; break;
-    case NPS_LEVEL_HYBRID: t1 = thr; t2 = bthr; t3 = gthr; break;
-    default: t1 = thr; t2 = thr; t3 = big; break;  // block
+    case NPS_LEVEL_WARP: tw = thr; tb = big; tg = big; break;
+    case NPS_LEVEL_BLOCK: tw = thr; tb = thr; tg = big; break;
+    case NPS_LEVEL_GRID: tw = thr; tb = thr; tg = thr; break;
+    default: tw = thr; tb = bthr; tg = gthr; break;  // hybrid
   }
 }
 
+// ---------------------------------------------------------------------------
 // Solve one instance with the CTAs of one team.  I refers to kernel-parameter
 // space (single-instance launches) or to a shared-memory copy (batches).
 template <int BS>
 __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS>& sm, uint32_t* bar,
-                               uint32_t& bar_epoch, uint32_t rank, uint32_t team_size,
-                               bool& inject) {
+                               uint32_t& bar_epoch, uint32_t rank, uint32_t team_size, bool& inject) {
+  constexpr int NW = BS / 32;
   Counters* ctr = I.ctr;
   const uint32_t gthreads = team_size * BS;
   const uint32_t gtid = rank * BS + threadIdx.x;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t gwarp = rank * NW + warp;
   const bool learned = I.policy == NPS_POLICY_LEARNED && P.policy != nullptr;
   const bool want_iter = learned || (I.trace != nullptr);
 
@@ -636,23 +790,25 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     // state mode: frontier = vertices with update[v] != 0 (cleared), distances kept
     const uint32_t nr = ((uint32_t)I.n + 31u) & ~31u;
     for (uint32_t v = gtid; v < nr; v += gthreads) {
-      bool f = false;
+      bool f[1] = {false};
       if (v < (uint32_t)I.n) {
-        f = I.update[v] != 0;
-        if (f) I.update[v] = 0;
+        f[0] = I.update[v] != 0;
+        if (f[0]) I.update[v] = 0;
         if (wrap) { I.mark[v] = 0; I.fmark[v] = 0; }
       }
-      append1(I.q[0], &ctr->qtail[0], I.qcap, f, (int32_t)v, &ctr->status, lane);
+      const int32_t vv[1] = {(int32_t)v};
+      append_k<1>(I.q[0], &ctr->qtail[0], I.qcap, f, vv, &ctr->status, lane);
     }
   }
-  if (rank == 0 && threadIdx.x == 0) {
-    ctr->fmin[0] = ctr->fmin[1] = ctr->fmin[2] = 0xffffffffu;
-  }
+  if (rank == 0 && threadIdx.x == 0) ctr->fmin[0] = ctr->fmin[1] = ctr->fmin[2] = 0xffffffffu;
+  if (threadIdx.x == 0) sm.blk_ctr = 0ull;
   const bool inj = inject;
   inject = false;
   if (!team_barrier<BS>(P, sm, bar, bar_epoch, team_size, &ctr->status, inj)) return;
 
-  uint32_t qlen = min(__ldcg(&ctr->qtail[0]), I.qcap);
+  if (threadIdx.x == 0) sm.bc_q = __ldcg(&ctr->qtail[0]);
+  __syncthreads();
+  uint32_t qlen = min(sm.bc_q, I.qcap);
   uint32_t it = 0, ep = 0;
   uint32_t delta = I.delta;
   uint32_t T = delta == 0 ? 0xffffffffu : delta;
@@ -682,48 +838,93 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     C.heavy = I.heavy + ((it & 1) ? hhalf : 0);
     C.heavy_ctr = &ctr->heavy[it % 3];
     C.hcap = hhalf;
-    level_thresholds(level, I.t1, I.t2, I.t3, C.t1, C.t2, C.t3);
+    level_thresholds(level, I.t1, I.t2, I.t3, C.t_warp, C.t_block, C.t_grid);
     const int4* Hprev = I.heavy + ((it & 1) ? 0 : hhalf);
 
-    if (rank == 0 && threadIdx.x == 0) {
-      ctr->qtail[(it + 2) % 3] = 0;
-      ctr->work[(it + 1) % 3] = 0;
-      ctr->heavy[(it + 1) % 3] = 0;
-      ctr->ftail[(E + 1) % 3] = 0;
-      ctr->fmin[(E + 1) % 3] = 0xffffffffu;
-      if (want_iter) {
-        const uint32_t sl = (it + 1) % 3;
-        for (int b = 0; b < 8; ++b) ctr->hist[sl][b] = 0;
-        ctr->it_edges[sl] = 0;
-        ctr->it_impr[sl] = 0;
-        ctr->it_reached[sl] = 0;
+    if (rank == 0 && threadIdx.x < kStripes) {
+      ctr->work[(it + 1) % 3][threadIdx.x * 32] = 0;
+      if (threadIdx.x == 0) {
+        ctr->qtail[(it + 2) % 3] = 0;
+        ctr->heavy[(it + 1) % 3] = 0;
+        ctr->ftail[(E + 1) % 3] = 0;
+        ctr->fmin[(E + 1) % 3] = 0xffffffffu;
+        if (want_iter) {
+          const uint32_t sl = (it + 1) % 3;
+          for (int b = 0; b < 8; ++b) ctr->hist[sl][b] = 0;
+          ctr->it_edges[sl] = 0;
+          ctr->it_impr[sl] = 0;
+          ctr->it_reached[sl] = 0;
+        }
       }
     }
     if (threadIdx.x < 8) sm.hist[threadIdx.x] = 0;
+    __syncthreads();
 
     const int32_t* srcq = advance ? I.fq[ep & 1] : I.q[it & 1];
     const uint32_t srclen = advance ? adv_len : qlen;
-    const uint32_t n_heavy_items = (uint32_t)((hprev_tot + BS - 1) / BS);
-    const uint32_t n_items = n_heavy_items + (srclen + BS - 1) / BS;
+    const uint32_t n_heavy_items = (uint32_t)((hprev_tot + kHeavyItemChunks - 1) / kHeavyItemChunks);
+    const uint32_t n_items = n_heavy_items + (srclen + 31) / 32;
     Acc acc = {0, 0, 0, 0};
+    Stage S;
+    S.nbuf = sm.stage[warp][0];
+    S.fbuf = sm.stage[warp][1];
+    S.ncnt = 0;
+    S.fcnt = 0;
 
-    // ---- work loop: dynamic items (grid-tier chunks first, then frontier chunks)
-    for (;;) {
-      if (threadIdx.x == 0) {
-        sm.item = atomicAdd(&ctr->work[it % 3], 1u);
-        sm.blk_ctr = 0ull;
+    // ---- warp work loop over striped counters: heavy chunk items, then vertex items.
+    // Warps beyond four per item stay out; an exhausted stripe is recognised by a
+    // plain read before any atomic is spent on it.
+    // The next item's index is requested before the current item is processed,
+    // so the atomic's round trip overlaps the work.
+    if ((unsigned long long)gwarp < 4ull * n_items + kStripes) {
+      uint32_t* wc = &ctr->work[it % 3][0];
+      int stripe = (int)(gwarp % kStripes);
+      uint32_t t_next = 0xffffffffu;
+      bool have_next = false;
+      for (int tried = 0; tried < kStripes;) {
+        const uint32_t stripe_items = n_items > (uint32_t)stripe ? (n_items - stripe + kStripes - 1) / kStripes : 0u;
+        uint32_t t = 0xffffffffu;
+        if (have_next) {
+          t = t_next;
+        } else if (lane == 0 && ld_relaxed_u32(&wc[stripe * 32]) < stripe_items) {
+          t = atomicAdd(&wc[stripe * 32], 1u);
+        }
+        t = __shfl_sync(kFull, t, 0);
+        have_next = false;
+        if (t >= stripe_items) {
+          stripe = (stripe + 1) % kStripes;
+          ++tried;
+          continue;
+        }
+        if (lane == 0) t_next = atomicAdd(&wc[stripe * 32], 1u);
+        have_next = true;
+        const unsigned long long item = (unsigned long long)t * kStripes + stripe;
+        if (item < n_heavy_items) {
+          const unsigned long long kb = item * kHeavyItemChunks;
+          const unsigned long long ke = min(kb + kHeavyItemChunks, hprev_tot);
+          walk_chunks(I, C, Hprev, hprev_cnt, kb, ke, acc, S, lane);
+        } else {
+          process_vertex_item<BS>(I, C, sm, srcq, (uint32_t)(item - n_heavy_items) * 32 + lane, srclen,
+                                  advance, T_old, want_iter, acc, S, lane);
+        }
       }
-      __syncthreads();
-      const uint32_t item = sm.item;
-      if (item >= n_items) break;
-      if (item < n_heavy_items) {
-        process_heavy<BS>(I, C, Hprev, hprev_cnt, hprev_tot, (unsigned long long)item * BS, acc);
-      } else {
-        process_vertices<BS>(I, C, sm, srcq, (item - n_heavy_items) * BS, srclen, advance, T_old,
-                             want_iter, acc);
-      }
-      __syncthreads();
     }
+
+    // ---- block tier: the CTA's warps walk the CTA list once
+    __syncthreads();
+    const uint32_t bcnt = min((uint32_t)(sm.blk_ctr >> 32), (uint32_t)kBlockListCap);
+    if (bcnt) {
+      // chunks of the stored entries only (overflowed entries were walked by their warp)
+      const int4 last = sm.blk[bcnt - 1];
+      const uint32_t btot = (uint32_t)last.w + row_chunks(last.x, last.y);
+      const uint32_t per = (btot + NW - 1) / NW;
+      const unsigned long long kb = (unsigned long long)warp * per;
+      const unsigned long long ke = min((unsigned long long)btot, kb + per);
+      walk_chunks(I, C, sm.blk, bcnt, kb, ke, acc, S, lane);
+      __syncthreads();
+      if (threadIdx.x == 0) sm.blk_ctr = 0ull;
+    }
+    stage_drain(S, C, I.qcap, &ctr->status, lane);
 
     // ---- per-CTA flush of iteration counters
     if (want_iter) {
@@ -750,10 +951,18 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
       ep += 1;
       buckets += 1;
     }
-    const uint32_t qn = min(__ldcg(&ctr->qtail[(it + 1) % 3]), I.qcap);
-    const unsigned long long hc = ld_relaxed_u64(&ctr->heavy[it % 3]);
+    // thread 0 reads the shared counters once per CTA and broadcasts them
+    if (threadIdx.x == 0) {
+      sm.bc_q = __ldcg(&ctr->qtail[(it + 1) % 3]);
+      sm.bc_h = ld_relaxed_u64(&ctr->heavy[it % 3]);
+      sm.bc_f = __ldcg(&ctr->ftail[ep % 3]);
+      sm.bc_m = __ldcg(&ctr->fmin[ep % 3]);
+    }
+    __syncthreads();
+    const uint32_t qn = min(sm.bc_q, I.qcap);
+    const unsigned long long hc = sm.bc_h;
     const uint32_t hn = min((uint32_t)(hc >> kHeavyShift), hhalf);
-    const uint32_t fl = min(__ldcg(&ctr->ftail[ep % 3]), I.qcap);
+    const uint32_t fl = min(sm.bc_f, I.qcap);
     const bool will_advance = qn == 0 && hn == 0 && fl != 0;
 
     if (want_iter) {
@@ -790,7 +999,8 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
         tr->edges = __ldcg(&ctr->it_edges[sl]);
         tr->improvements = __ldcg(&ctr->it_impr[sl]);
         tr->reached = reached_total;
-        tr->pad = hn;
+        tr->heavy = hn;
+        tr->t_ns = globaltimer_ns() - sm.t_start;
       }
     }
 
@@ -804,7 +1014,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
       }
       // bucket advance: the next iteration filters the far pile of epoch ep
       if (learned) delta = 1u << sm.pol_choice[0];
-      const uint32_t fm = __ldcg(&ctr->fmin[ep % 3]);
+      const uint32_t fm = sm.bc_m;
       const uint32_t dstep = delta ? delta : 1u;
       unsigned long long nt = (unsigned long long)T + dstep;
       if (fm != 0xffffffffu && (unsigned long long)fm + dstep > nt) nt = (unsigned long long)fm + dstep;
@@ -833,11 +1043,16 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
   }
 }
 
+// Resident CTAs per SM the register budget is sized for (about 768-1024
+// threads per SM: enough warps in flight to cover L2 and HBM latency).
+template <int BS>
+constexpr int kMinBlocks = BS >= 512 ? 2 : (BS >= 256 ? 3 : 6);
+
 // The persistent kernel.  SINGLE: one instance whose descriptor is the kernel
 // parameter `single` (constant-bank reads in the hot loops); otherwise the
 // team's instances are staged one at a time in shared memory.
 template <int BS, bool SINGLE>
-__global__ void __launch_bounds__(BS) sssp_persistent_kernel(const __grid_constant__ LaunchParams P,
+__global__ void __launch_bounds__(BS, kMinBlocks<BS>) sssp_persistent_kernel(const __grid_constant__ LaunchParams P,
                                                              const __grid_constant__ InstDesc single) {
   __shared__ Smem<BS> sm;
   __shared__ InstDesc sinst;
@@ -856,23 +1071,24 @@ __global__ void __launch_bounds__(BS) sssp_persistent_kernel(const __grid_consta
   __syncthreads();
   if (sm.team_id < 0) return;
   const TeamDesc td = sm.team;
-  uint32_t* bar = P.bar + 32 * sm.team_id;
+  uint32_t* bar = P.bar + (size_t)P.bar_stride * sm.team_id;
   uint32_t bar_epoch = 0;
   const uint32_t rank = blockIdx.x - td.cta_begin;
+  if (threadIdx.x == 0) sm.rank = rank;
+  __syncthreads();
   bool inject = P.fault_inject_wait != 0;
   if constexpr (SINGLE) {
     solve_instance<BS>(P, single, sm, bar, bar_epoch, rank, (uint32_t)td.cta_count, inject);
-    return;
   } else {
-  for (int k = 0; k < td.inst_count; ++k) {
-    __syncthreads();
-    if (threadIdx.x == 0) sinst = P.inst[P.order[td.inst_begin + k]];
-    __syncthreads();
-    solve_instance<BS>(P, sinst, sm, bar, bar_epoch, rank, (uint32_t)td.cta_count, inject);
-    if (ld_relaxed_u32(P.abort_flag)) return;
-    // instances of a team are separated by a barrier so every CTA sees the previous one done
-    if (!team_barrier<BS>(P, sm, bar, bar_epoch, (uint32_t)td.cta_count, &sinst.ctr->status, false)) return;
-  }
+    for (int k = 0; k < td.inst_count; ++k) {
+      __syncthreads();
+      if (threadIdx.x == 0) sinst = P.inst[P.order[td.inst_begin + k]];
+      __syncthreads();
+      solve_instance<BS>(P, sinst, sm, bar, bar_epoch, rank, (uint32_t)td.cta_count, inject);
+      if (ld_relaxed_u32(P.abort_flag)) return;
+      // instances of a team are separated by a barrier so every CTA sees the previous one done
+      if (!team_barrier<BS>(P, sm, bar, bar_epoch, (uint32_t)td.cta_count, &sinst.ctr->status, false)) return;
+    }
   }
 }
 

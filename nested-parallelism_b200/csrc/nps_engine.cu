@@ -171,14 +171,21 @@ struct DevBuf {
 };
 
 // Control block: counters, barrier words and the abort flag share one
-// allocation so a single memset clears them before each launch.
+// allocation so a single memset clears them before each launch.  Layout:
+//   Counters[n_inst] | barrier words, `stride` per team | abort flag (128 B) | team table (128 B)
 struct Control {
-  size_t n_inst = 0, n_teams = 0;
+  size_t n_inst = 0, n_teams = 0, stride = 0;
   char* base = nullptr;
-  size_t bytes = 0;
+  Control(size_t ni, size_t nt, int max_team_ctas)
+      : n_inst(ni), n_teams(nt), stride(32 * (2 + (size_t)(max_team_ctas + nps::kBarGroup - 1) / nps::kBarGroup)) {}
+  size_t counters_bytes() const { return n_inst * sizeof(Counters); }
+  size_t bar_bytes() const { return n_teams * stride * sizeof(uint32_t); }
   Counters* ctr() const { return (Counters*)base; }
-  uint32_t* bar() const { return (uint32_t*)(base + n_inst * sizeof(Counters)); }
-  uint32_t* abort_flag() const { return bar() + 32 * n_teams; }
+  uint32_t* bar() const { return (uint32_t*)(base + counters_bytes()); }
+  uint32_t* abort_flag() const { return (uint32_t*)(base + counters_bytes() + bar_bytes()); }
+  TeamDesc* team_table() const { return (TeamDesc*)(base + counters_bytes() + bar_bytes() + 128); }
+  size_t clear_bytes() const { return counters_bytes() + bar_bytes() + 128; }
+  size_t bytes() const { return clear_bytes() + 128; }
 };
 
 struct PolicyState {
@@ -382,18 +389,15 @@ nps_status run_single(nps_ctx* c, cudaStream_t s, const int32_t* row, const int3
   if (grow_marks) NPS_CUDA(cudaMemsetAsync(c->stamp.p, 0, sizeof(uint32_t), s));
   const uint32_t hcap = heavy_capacity(n, m, p);
   if ((e = c->heavy.ensure(hcap, false, s))) return e;
-  Control ctl;
-  ctl.n_inst = 1;
-  ctl.n_teams = 1;
-  ctl.bytes = sizeof(Counters) + 32 * sizeof(uint32_t) + 128;
-  if ((e = c->control.ensure(ctl.bytes, false, s))) return e;
+  int grid = 0;
+  if ((e = grid_size(c->device, c->di, p.block_size, true, p.ctas_per_sm, &grid))) return e;
+  Control ctl(1, 1, grid);
+  if ((e = c->control.ensure(ctl.bytes(), false, s))) return e;
   ctl.base = c->control.p;
   if (p.trace) {
     if ((e = c->trace.ensure(1 << 16, false, s))) return e;
   }
   if ((e = ensure_pinned_counters(c, 1))) return e;
-  int grid = 0;
-  if ((e = grid_size(c->device, c->di, p.block_size, true, p.ctas_per_sm, &grid))) return e;
 
   InstDesc d;
   memset(&d, 0, sizeof(d));
@@ -432,17 +436,17 @@ nps_status run_single(nps_ctx* c, cudaStream_t s, const int32_t* row, const int3
   lp.n_teams = 1;
   lp.fault_inject_wait = p.reserved[0] != 0;
   lp.bar = ctl.bar();
+  lp.bar_stride = (uint32_t)ctl.stride;
   lp.abort_flag = ctl.abort_flag();
   lp.timeout_ns = (unsigned long long)(p.timeout_s * 1e9);
   lp.run_budget_ns = run_budget_ns(p);
   lp.policy = policy_ptr(c->device);
   if (p.policy == NPS_POLICY_LEARNED && !lp.policy)
     return nps_fail(NPS_ERR_INVALID_ARG, "learned policy requested but no weights loaded (nps_policy_set_weights)");
-  // the team table lives after the abort flag in the control block
-  TeamDesc* d_team = (TeamDesc*)(ctl.abort_flag() + 16);
+  TeamDesc* d_team = ctl.team_table();
   lp.teams = d_team;
 
-  NPS_CUDA(cudaMemsetAsync(ctl.base, 0, ctl.bytes - 128 + 64, s));
+  NPS_CUDA(cudaMemsetAsync(ctl.base, 0, ctl.clear_bytes(), s));
   NPS_CUDA(cudaMemcpyAsync(d_team, &td, sizeof(td), cudaMemcpyHostToDevice, s));
   if (time_it) NPS_CUDA(cudaEventRecord(c->ev[1], s));
   if ((e = launch(c, s, p.block_size, true, grid, lp, d))) return e;
@@ -642,10 +646,7 @@ extern "C" nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, co
                     memcmp(c->b_key.data(), inst, sizeof(nps_instance) * count) == 0 &&
                     memcmp(&c->b_params_key, &p, sizeof(p)) == 0;
   const int nteams = std::min(count, grid);
-  Control ctl;
-  ctl.n_inst = (size_t)count;
-  ctl.n_teams = (size_t)nteams;
-  ctl.bytes = sizeof(Counters) * (size_t)count + 32 * sizeof(uint32_t) * (size_t)nteams + 128;
+  Control ctl((size_t)count, (size_t)nteams, grid);
 
   if (!same) {
     if (c->b_graph) cudaGraphExecDestroy(c->b_graph);
@@ -665,7 +666,7 @@ extern "C" nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, co
     if ((e = c->b_stamp.ensure(mk_total + (size_t)count, true, s))) return e;
     if (!regrow) NPS_CUDA(cudaMemsetAsync(c->b_stamp.p, 0, sizeof(uint32_t) * (mk_total + count), s));
     if ((e = c->b_heavy.ensure(h_total, false, s))) return e;
-    if ((e = c->b_control.ensure(ctl.bytes, false, s))) return e;
+    if ((e = c->b_control.ensure(ctl.bytes(), false, s))) return e;
     if ((e = c->b_inst.ensure((size_t)count, false, s))) return e;
     if ((e = c->b_teams.ensure((size_t)nteams, false, s))) return e;
     if ((e = c->b_order.ensure((size_t)count, false, s))) return e;
@@ -764,6 +765,7 @@ extern "C" nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, co
   lp.n_teams = c->b_nteams;
   lp.fault_inject_wait = p.reserved[0] != 0;
   lp.bar = ctl.bar();
+  lp.bar_stride = (uint32_t)ctl.stride;
   lp.abort_flag = ctl.abort_flag();
   lp.timeout_ns = (unsigned long long)(p.timeout_s * 1e9);
   lp.run_budget_ns = run_budget_ns(p);
@@ -779,7 +781,7 @@ extern "C" nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, co
     if (!c->b_graph) {
       cudaGraph_t g = nullptr;
       NPS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-      cudaError_t ce = cudaMemsetAsync(ctl.base, 0, ctl.bytes - 64, s);
+      cudaError_t ce = cudaMemsetAsync(ctl.base, 0, ctl.clear_bytes(), s);
       nps_status le = ce == cudaSuccess ? launch(c, s, p.block_size, false, grid, lp, dummy) : NPS_ERR_CUDA;
       cudaError_t ee = cudaStreamEndCapture(s, &g);
       if (ce != cudaSuccess) return nps_fail(NPS_ERR_CUDA, std::string("capture memset: ") + cudaGetErrorString(ce));
@@ -798,7 +800,7 @@ extern "C" nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, co
     }
     NPS_CUDA(cudaGraphLaunch(c->b_graph, s));
   } else {
-    NPS_CUDA(cudaMemsetAsync(ctl.base, 0, ctl.bytes - 64, s));
+    NPS_CUDA(cudaMemsetAsync(ctl.base, 0, ctl.clear_bytes(), s));
     if ((e = launch(c, s, p.block_size, false, grid, lp, dummy))) return e;
   }
   NPS_CUDA(cudaEventRecord(c->ev[2], s));
