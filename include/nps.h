@@ -86,7 +86,10 @@ typedef struct nps_params {
   void* stream;             /* cudaStream_t to launch on; NULL = the library's own stream */
   double timeout_s;         /* bound on every spin wait inside the persistent kernel (default 10 s) */
   int32_t trace;            /* 1: record one nps_trace_rec per iteration (read with nps_trace_read) */
-  int32_t reserved[7];
+  int32_t light_heavy;      /* 1 (default): with delta > 0, edges of weight >= delta are relaxed once,
+                               when the bucket that settles their tail drains (Meyer-Sanders split) */
+  int32_t reserved[6];      /* reserved[0] = 1: test hook, the first in-kernel barrier waits for an
+                               arrival that never comes, so its bounded wait must expire */
 } nps_params;
 
 typedef struct nps_stats {
@@ -102,6 +105,12 @@ typedef struct nps_stats {
   float total_ms;           /* device time including copies done by the call */
   int32_t status;           /* device status word */
   int32_t grid_ctas;        /* CTAs in the persistent launch */
+  /* SM cycles summed over warps per phase of the persistent loop; filled only by
+   * a library built with -DNPS_PROFILE (zero otherwise):
+   * 0 work-item fetch, 1 vertex loads + classification, 2 small-row rounds,
+   * 3 warp-tier rows, 4 grid-tier chunk walk, 5 block-tier walk, 6 staging drain,
+   * 7 team barrier, 8 iteration bookkeeping */
+  uint64_t phase_cycles[9];
 } nps_stats;
 
 /* One record per frontier iteration when nps_params.trace = 1. */

@@ -192,6 +192,7 @@ class Params:
     device: int = 0
     timeout_s: float = 10.0
     trace: bool = False
+    light_heavy: bool = True            # delta > 0: heavy edges (w >= delta) relaxed once per bucket
     fault_inject_wait: bool = False     # test hook: the first barrier can never complete
 
     def to_c(self, device_ptrs: bool, stream: Optional[int] = None) -> nps_params:
@@ -202,6 +203,7 @@ class Params:
         p.block_size, p.ctas_per_sm, p.delta = self.block_size, self.ctas_per_sm, self.delta
         p.policy, p.device, p.timeout_s = self.policy, self.device, float(self.timeout_s)
         p.trace = int(bool(self.trace))
+        p.light_heavy = int(bool(self.light_heavy))
         p.device_ptrs = int(bool(device_ptrs))
         p.stream = stream
         p.reserved[0] = int(bool(self.fault_inject_wait))
@@ -220,12 +222,13 @@ class Stats:
     total_ms: float = 0.0
     status: int = 0
     grid_ctas: int = 0
+    phase_cycles: tuple = ()
 
     @staticmethod
     def from_c(s: nps_stats) -> "Stats":
         return Stats(int(s.iterations), int(s.buckets), int(s.edges_scanned), int(s.improvements),
                      int(s.vertices_processed), int(s.reached), float(s.kernel_ms), float(s.total_ms),
-                     int(s.status), int(s.grid_ctas))
+                     int(s.status), int(s.grid_ctas), tuple(int(x) for x in s.phase_cycles))
 
 
 def _ptr(x) -> int:

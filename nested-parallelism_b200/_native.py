@@ -34,7 +34,7 @@ class nps_params(C.Structure):
         ("grid_threshold", C.c_int32), ("block_size", C.c_int32), ("ctas_per_sm", C.c_int32),
         ("delta", C.c_uint32), ("policy", C.c_int32), ("device_ptrs", C.c_int32),
         ("device", C.c_int32), ("stream", C.c_void_p), ("timeout_s", C.c_double),
-        ("trace", C.c_int32), ("reserved", C.c_int32 * 7),
+        ("trace", C.c_int32), ("light_heavy", C.c_int32), ("reserved", C.c_int32 * 6),
     ]
 
 
@@ -44,6 +44,7 @@ class nps_stats(C.Structure):
         ("improvements", C.c_uint64), ("vertices_processed", C.c_uint64), ("reached", C.c_uint32),
         ("pad0", C.c_uint32), ("reached_edges", C.c_uint64), ("kernel_ms", C.c_float),
         ("total_ms", C.c_float), ("status", C.c_int32), ("grid_ctas", C.c_int32),
+        ("phase_cycles", C.c_uint64 * 9),
     ]
 
 

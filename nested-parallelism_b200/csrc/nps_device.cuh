@@ -57,7 +57,7 @@ constexpr uint32_t kInf = NPS_INF;
 constexpr int kHeavyShift = 36;  // heavy counter packs (count << 36) | chunk_offset
 constexpr unsigned long long kHeavyMask = (1ull << kHeavyShift) - 1;
 constexpr int kStripes = 8;            // striped work counters
-constexpr int kHeavyItemChunks = 128;  // chunks (4 edges each) per heavy work item
+constexpr int kHeavyItemChunks = 64;   // chunks (4 edges each) per heavy work item
 constexpr int kBlockListCap = 512;     // CTA list entries (block tier)
 
 // Per-instance device counters.  Zeroed by the host before a launch.
@@ -65,6 +65,7 @@ struct __align__(128) Counters {
   uint32_t qtail[3];   // near-queue tails, slot = iteration % 3
   uint32_t ftail[3];   // far-pile tails,   slot = epoch % 3
   uint32_t fmin[3];    // min distance pushed into the far pile on an advance, slot = epoch % 3
+  uint32_t stail[3];   // settle-list tails, slot = heavy generation % 3
   uint32_t status;     // NPS_OK or the first error
   unsigned long long heavy[3];  // grid-tier list counter, slot = iteration % 3
   uint32_t iterations;
@@ -80,6 +81,8 @@ struct __align__(128) Counters {
   unsigned long long it_impr[3];
   uint32_t it_reached[3];
   uint32_t pad1[3];
+  unsigned long long prof[9];   // NPS_PROFILE builds: SM cycles per phase, summed over warps
+  unsigned long long pad2[7];
   // striped work counters, one 128-byte line each: work[slot][stripe * 32]
   uint32_t work[3][kStripes * 32];
 };
@@ -98,7 +101,9 @@ struct InstDesc {
   int32_t* fq[2];       // far piles   (capacity qcap)
   uint32_t* mark;       // near-queue dedupe stamps
   uint32_t* fmark;      // far-pile dedupe stamps
-  int4* heavy;          // grid-tier entries {row start, row end, vertex, chunk offset}
+  int4* heavy;          // grid-tier entries {row start, row end, vertex | heavy flag, chunk offset}
+  int32_t* sq[2];       // settle lists (light/heavy split): vertices processed in the bucket
+  uint32_t* smark;      // settle-list dedupe stamps
   uint32_t qcap;
   uint32_t hcap;
   Counters* ctr;
@@ -110,7 +115,7 @@ struct InstDesc {
   int32_t t1, t2, t3;   // threshold, block_threshold, grid_threshold
   int32_t policy;
   int32_t vec_ok;       // col / w are 16-byte aligned
-  int32_t pad0;
+  int32_t light_heavy;  // 1: split edges at delta (relax w >= delta once per settled vertex)
 };
 
 struct TeamDesc {
@@ -235,7 +240,18 @@ struct IterCtx {
   int32_t t_warp;    // degree >= t_warp leaves the small path
   int32_t t_block;   // degree >= t_block goes to the CTA list
   int32_t t_grid;    // degree >= t_grid goes to H
+  uint32_t split;    // light/heavy split weight (0: no split, every edge is relaxed)
+  bool heavy_iter;   // this iteration relaxes heavy edges of the settle list
+  int32_t* sq;       // settle list receiving processed vertices (null: no settle appends)
+  uint32_t* sq_tail;
+  uint32_t sstamp;
 };
+
+// Whether an edge of weight w is relaxed by a pass over light (heavy = false)
+// or heavy (heavy = true) edges.
+__device__ __forceinline__ bool edge_in_pass(const IterCtx& C, uint32_t w, bool heavy) {
+  return C.split == 0u || (heavy ? w >= C.split : w < C.split);
+}
 
 // Thread-local accumulators, reduced per CTA.
 struct Acc {
@@ -244,6 +260,31 @@ struct Acc {
   uint32_t reached;
   uint32_t processed;
 };
+
+// Phase timers of an NPS_PROFILE build: each warp's lane 0 sums clock64()
+// deltas per phase; the sums reach Counters::prof at the end of the launch.
+#ifdef NPS_PROFILE
+struct PhaseClock {
+  unsigned long long acc[9];
+  long long t;
+  __device__ __forceinline__ void reset() {
+    for (int i = 0; i < 9; ++i) acc[i] = 0;
+    t = clock64();
+  }
+  __device__ __forceinline__ void lap(int phase) {
+    const long long now = clock64();
+    acc[phase] += (unsigned long long)(now - t);
+    t = now;
+  }
+};
+#define NPS_LAP(pc, phase) (pc).lap(phase)
+#else
+struct PhaseClock {
+  __device__ __forceinline__ void reset() {}
+  __device__ __forceinline__ void lap(int) {}
+};
+#define NPS_LAP(pc, phase) ((void)0)
+#endif
 
 // ---------------------------------------------------------------------------
 // Batched relaxation: K candidate edges per lane.  All K distance loads are
@@ -284,13 +325,12 @@ __device__ __forceinline__ void relax_batch(const InstDesc& I, const IterCtx& C,
     if (go[j] && nd[j] < old[j]) {
       acc.impr++;
       if (old[j] == kInf) acc.reached++;
+      // one exchange decides whether this improvement is the first of the iteration
       if (nd[j] < C.T) {
-        if (__ldcg(I.mark + v[j]) != C.snear) pn[j] = atomicExch(I.mark + v[j], C.snear) != C.snear;
+        pn[j] = atomicExch(I.mark + v[j], C.snear) != C.snear;
       } else {
-        if (__ldcg(I.fmark + v[j]) != C.sfar) {
-          pf[j] = atomicExch(I.fmark + v[j], C.sfar) != C.sfar;
-          if (pf[j] && C.fp_min) atomicMin(C.fp_min, nd[j]);
-        }
+        pf[j] = atomicExch(I.fmark + v[j], C.sfar) != C.sfar;
+        if (pf[j] && C.fp_min) atomicMin(C.fp_min, nd[j]);
       }
     }
   }
@@ -330,13 +370,15 @@ __device__ __forceinline__ void append_k(int32_t* q, uint32_t* tail, uint32_t ca
 // vertices it pushes and moves them to the global queue 32 at a time (one
 // atomicAdd on the queue tail per >= 32 entries, one coalesced 128-byte store
 // per 32), so warps do not serialise on the tail counter every round.
-constexpr int kStage = 192;  // >= 31 left over + 4 * 32 from one append
+constexpr int kStage = 160;  // >= 31 left over + 4 * 32 from one append
 
 struct Stage {
   int32_t* nbuf;   // near-queue staging (kStage entries, shared memory)
   int32_t* fbuf;   // far-pile staging
+  int32_t* sbuf;   // settle-list staging
   uint32_t ncnt;   // warp-uniform fill counts
   uint32_t fcnt;
+  uint32_t scnt;
 };
 
 // Move the first `nflush` staged entries to q and shift the rest down.
@@ -385,6 +427,7 @@ __device__ __forceinline__ void stage_k(int32_t* buf, uint32_t& cnt, const bool 
 __device__ __forceinline__ void stage_drain(Stage& S, const IterCtx& C, uint32_t qcap, uint32_t* status, int lane) {
   if (S.ncnt) stage_flush(S.nbuf, S.ncnt, S.ncnt, C.qn, C.qn_tail, qcap, status, lane);
   if (S.fcnt) stage_flush(S.fbuf, S.fcnt, S.fcnt, C.fp, C.fp_tail, qcap, status, lane);
+  if (S.scnt) stage_flush(S.sbuf, S.scnt, S.scnt, C.sq, C.sq_tail, qcap, status, lane);
 }
 
 template <int K>
@@ -417,13 +460,15 @@ __device__ __forceinline__ void load_chunk(const InstDesc& I, bool act, int32_t 
   }
 }
 
-// Relax the edges of chunk c that fall inside [s, e).  Warp-collective.
-__device__ __forceinline__ void relax_chunk(const InstDesc& I, const IterCtx& C, bool act, int32_t c,
-                                            int32_t s, int32_t e, uint32_t du, Acc& acc, Stage& S, int lane) {
-  int4 cv, wv;
-  load_chunk(I, act, c, s, e, cv, wv);
-  const bool valid[4] = {act && c >= s && c < e, act && c + 1 >= s && c + 1 < e,
-                         act && c + 2 >= s && c + 2 < e, act && c + 3 >= s && c + 3 < e};
+// Relax the edges of an already loaded chunk c that fall inside [s, e).
+// Warp-collective.
+__device__ __forceinline__ void relax_loaded(const InstDesc& I, const IterCtx& C, bool act, int32_t c,
+                                             int32_t s, int32_t e, uint32_t du, bool heavy, const int4& cv,
+                                             const int4& wv, Acc& acc, Stage& S, int lane) {
+  const bool valid[4] = {act && c >= s && c < e && edge_in_pass(C, (uint32_t)wv.x, heavy),
+                         act && c + 1 >= s && c + 1 < e && edge_in_pass(C, (uint32_t)wv.y, heavy),
+                         act && c + 2 >= s && c + 2 < e && edge_in_pass(C, (uint32_t)wv.z, heavy),
+                         act && c + 3 >= s && c + 3 < e && edge_in_pass(C, (uint32_t)wv.w, heavy)};
   const int32_t v[4] = {cv.x, cv.y, cv.z, cv.w};
   const uint32_t nd[4] = {tent(du, (uint32_t)wv.x), tent(du, (uint32_t)wv.y), tent(du, (uint32_t)wv.z),
                           tent(du, (uint32_t)wv.w)};
@@ -439,7 +484,7 @@ struct Smem {
   int32_t ok;
   uint32_t hist[8];
   int4 blk[kBlockListCap];     // block-tier entries {s, e, vertex, chunk offset}
-  int32_t stage[BS / 32][2][kStage];  // per-warp append staging: [near, far]
+  int32_t stage[BS / 32][3][kStage];  // per-warp append staging: [near, far, settle]
   uint32_t red[4][BS / 32];
   float feat[NPS_MLP_IN];
   float hid[NPS_MLP_HID];
@@ -447,7 +492,7 @@ struct Smem {
   TeamDesc team;
   int32_t team_id;
   uint32_t rank;
-  uint32_t bc_q, bc_f, bc_m;   // counters broadcast after a barrier
+  uint32_t bc_q, bc_f, bc_m, bc_s;   // counters broadcast after a barrier
   unsigned long long bc_h;
   unsigned long long t_start;
 };
@@ -545,7 +590,9 @@ __device__ __forceinline__ void warp_row(const InstDesc& I, const IterCtx& C, in
                                          Acc& acc, Stage& S, int lane) {
   for (int32_t c0 = s & ~3; c0 < e; c0 += 128) {
     const int32_t c = c0 + lane * 4;
-    relax_chunk(I, C, c < e, c, s, e, du, acc, S, lane);
+    int4 cv, wv;
+    load_chunk(I, c < e, c, s, e, cv, wv);
+    relax_loaded(I, C, c < e, c, s, e, du, C.heavy_iter, cv, wv, acc, S, lane);
   }
 }
 
@@ -555,7 +602,7 @@ template <int BS>
 __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const IterCtx& C, Smem<BS>& sm,
                                                     const int32_t* src_q, uint32_t idx, uint32_t src_len,
                                                     bool advance, uint32_t T_old, bool want_hist, Acc& acc,
-                                                    Stage& S, int lane) {
+                                                    Stage& S, PhaseClock& pc, int lane) {
   int32_t v = -1, s = 0, e = 0;
   uint32_t du = 0;
   bool repush = false;
@@ -593,6 +640,15 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
     stage_k<1>(S.fbuf, S.fcnt, f, vv, C.fp, C.fp_tail, I.qcap, &I.ctr->status, lane);
   }
   const int32_t deg = e - s;
+  if (C.sq) {
+    // light pass: the vertex joins the bucket's settle list once, for its heavy edges
+    bool f[1] = {false};
+    if (deg > 0 && __ldcg(I.smark + v) != C.sstamp) f[0] = atomicExch(I.smark + v, C.sstamp) != C.sstamp;
+    const int32_t vv[1] = {v};
+    stage_k<1>(S.sbuf, S.scnt, f, vv, C.sq, C.sq_tail, I.qcap, &I.ctr->status, lane);
+  }
+  // deferred entries remember which edges they relax in the top bit of the vertex id
+  const int32_t vtag = C.heavy_iter ? (int32_t)((uint32_t)v | 0x80000000u) : v;
   const bool small = deg > 0 && deg < C.t_warp;
   bool wtier = deg >= C.t_warp && deg < C.t_block;
   const bool btier = deg >= C.t_block && deg < C.t_grid;
@@ -601,17 +657,18 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
     // slot and chunk offset from one atomic, so offsets increase with the slot
     const unsigned long long old = atomicAdd(&sm.blk_ctr, (1ull << 32) | row_chunks(s, e));
     const uint32_t slot = (uint32_t)(old >> 32);
-    if (slot < (uint32_t)kBlockListCap) sm.blk[slot] = make_int4(s, e, v, (int32_t)(uint32_t)old);
+    if (slot < (uint32_t)kBlockListCap) sm.blk[slot] = make_int4(s, e, vtag, (int32_t)(uint32_t)old);
     else wtier = true;  // CTA list full: the warp walks the row itself
   }
   if (gtier) {
     const uint32_t nch = row_chunks(s, e);
     const unsigned long long old = atomicAdd(C.heavy_ctr, (1ull << kHeavyShift) | nch);
     const uint32_t slot = (uint32_t)(old >> kHeavyShift);
-    if (slot < C.hcap) C.heavy[slot] = make_int4(s, e, v, (int32_t)(uint32_t)(old & kHeavyMask));
+    if (slot < C.hcap) C.heavy[slot] = make_int4(s, e, vtag, (int32_t)(uint32_t)(old & kHeavyMask));
     else atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_CAPACITY);
   }
 
+  NPS_LAP(pc, 1);
   // ---- small rows: warp-flat loop, four edges per lane per round
   {
     const uint32_t d = small ? (uint32_t)deg : 0u;
@@ -650,11 +707,15 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
         nd[j] = valid[j] ? (uint32_t)ld_stream((const int32_t*)I.w + ei[j]) : 0u;
       }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) nd[j] = tent(dj[j], nd[j]);
+      for (int j = 0; j < 4; ++j) {
+        valid[j] = valid[j] && edge_in_pass(C, nd[j], C.heavy_iter);
+        nd[j] = tent(dj[j], nd[j]);
+      }
       relax_and_push<4>(I, C, valid, nb, nd, acc, S, lane);
     }
   }
 
+  NPS_LAP(pc, 2);
   // ---- warp tier: the warp walks each of its rows
   {
     uint32_t wb = __ballot_sync(kFull, wtier);
@@ -667,6 +728,7 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
       warp_row(I, C, rs, re, rdu, acc, S, lane);
     }
   }
+  NPS_LAP(pc, 3);
 }
 
 // Flat chunk-space walk of a list of rows {s, e, vertex, chunk offset} sorted by
@@ -688,10 +750,10 @@ __device__ __forceinline__ void walk_chunks(const InstDesc& I, const IterCtx& C,
   int j = lo;
   int4 ent = L[j];
   uint32_t nxt = (j + 1 < (int)cnt) ? (uint32_t)L[j + 1].w : 0xffffffffu;
-  // the owner's distance is read when the owner changes; a value that has
+  // The owner's distance is read when the owner changes.  A value that has
   // dropped since only makes this walk relax with a larger tentative distance,
-  // and the owner is back in a queue for every drop
-  uint32_t du = (k < k_end) ? __ldcg(I.dist + ent.z) : 0u;
+  // and the owner is back in a queue for every drop.
+  uint32_t du = (k < k_end) ? __ldcg(I.dist + (ent.z & 0x7fffffff)) : 0u;
   for (unsigned long long k0 = k_begin; k0 < k_end; k0 += 32) {
     k = k0 + lane;
     const bool act = k < k_end;
@@ -702,9 +764,11 @@ __device__ __forceinline__ void walk_chunks(const InstDesc& I, const IterCtx& C,
       nxt = (j + 1 < (int)cnt) ? (uint32_t)L[j + 1].w : 0xffffffffu;
       moved = true;
     }
-    if (moved) du = __ldcg(I.dist + ent.z);
+    if (moved) du = __ldcg(I.dist + (ent.z & 0x7fffffff));
     const int32_t c = (ent.x & ~3) + 4 * (int32_t)(k - (uint32_t)ent.w);
-    relax_chunk(I, C, act, c, ent.x, ent.y, du, acc, S, lane);
+    int4 cv, wv;
+    load_chunk(I, act, c, ent.x, ent.y, cv, wv);
+    relax_loaded(I, C, act, c, ent.x, ent.y, du, ent.z < 0, cv, wv, acc, S, lane);
   }
 }
 
@@ -780,7 +844,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
   if (I.mode == 0) {
     for (uint32_t v = gtid; v < (uint32_t)I.n; v += gthreads) {
       I.dist[v] = (v == (uint32_t)I.src) ? 0u : kInf;
-      if (wrap) { I.mark[v] = 0; I.fmark[v] = 0; }
+      if (wrap) { I.mark[v] = 0; I.fmark[v] = 0; I.smark[v] = 0; }
     }
     if (rank == 0 && threadIdx.x == 0) {
       I.q[0][0] = I.src;
@@ -794,7 +858,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
       if (v < (uint32_t)I.n) {
         f[0] = I.update[v] != 0;
         if (f[0]) I.update[v] = 0;
-        if (wrap) { I.mark[v] = 0; I.fmark[v] = 0; }
+        if (wrap) { I.mark[v] = 0; I.fmark[v] = 0; I.smark[v] = 0; }
       }
       const int32_t vv[1] = {(int32_t)v};
       append_k<1>(I.q[0], &ctr->qtail[0], I.qcap, f, vv, &ctr->status, lane);
@@ -813,11 +877,16 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
   uint32_t delta = I.delta;
   uint32_t T = delta == 0 ? 0xffffffffu : delta;
   bool advance = false;
+  bool heavy_it = false;  // this iteration relaxes the heavy edges of the settle list
+  uint32_t hg = 0;        // settle-list generation
+  uint32_t slen = 0;
   uint32_t adv_len = 0, T_old = 0;
   uint32_t hprev_cnt = 0;
   unsigned long long hprev_tot = 0;
   int level = I.level;
   Acc tot = {0, 0, 0, 0};
+  PhaseClock pc;
+  pc.reset();
   uint32_t buckets = 0;
   uint32_t reached_total = 1;
   const uint32_t hhalf = I.hcap / 2;
@@ -838,6 +907,11 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     C.heavy = I.heavy + ((it & 1) ? hhalf : 0);
     C.heavy_ctr = &ctr->heavy[it % 3];
     C.hcap = hhalf;
+    C.split = (I.light_heavy && delta != 0) ? delta : 0u;
+    C.heavy_iter = heavy_it;
+    C.sq = (C.split != 0u && !heavy_it) ? I.sq[hg & 1] : nullptr;
+    C.sq_tail = &ctr->stail[hg % 3];
+    C.sstamp = base + hg + 1;
     level_thresholds(level, I.t1, I.t2, I.t3, C.t_warp, C.t_block, C.t_grid);
     const int4* Hprev = I.heavy + ((it & 1) ? 0 : hhalf);
 
@@ -848,6 +922,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
         ctr->heavy[(it + 1) % 3] = 0;
         ctr->ftail[(E + 1) % 3] = 0;
         ctr->fmin[(E + 1) % 3] = 0xffffffffu;
+        if (heavy_it) ctr->stail[(hg + 1) % 3] = 0;
         if (want_iter) {
           const uint32_t sl = (it + 1) % 3;
           for (int b = 0; b < 8; ++b) ctr->hist[sl][b] = 0;
@@ -860,16 +935,18 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     if (threadIdx.x < 8) sm.hist[threadIdx.x] = 0;
     __syncthreads();
 
-    const int32_t* srcq = advance ? I.fq[ep & 1] : I.q[it & 1];
-    const uint32_t srclen = advance ? adv_len : qlen;
+    const int32_t* srcq = advance ? I.fq[ep & 1] : (heavy_it ? I.sq[hg & 1] : I.q[it & 1]);
+    const uint32_t srclen = advance ? adv_len : (heavy_it ? slen : qlen);
     const uint32_t n_heavy_items = (uint32_t)((hprev_tot + kHeavyItemChunks - 1) / kHeavyItemChunks);
     const uint32_t n_items = n_heavy_items + (srclen + 31) / 32;
     Acc acc = {0, 0, 0, 0};
     Stage S;
     S.nbuf = sm.stage[warp][0];
     S.fbuf = sm.stage[warp][1];
+    S.sbuf = sm.stage[warp][2];
     S.ncnt = 0;
     S.fcnt = 0;
+    S.scnt = 0;
 
     // ---- warp work loop over striped counters: heavy chunk items, then vertex items.
     // Warps beyond four per item stay out; an exhausted stripe is recognised by a
@@ -899,17 +976,20 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
         if (lane == 0) t_next = atomicAdd(&wc[stripe * 32], 1u);
         have_next = true;
         const unsigned long long item = (unsigned long long)t * kStripes + stripe;
+        NPS_LAP(pc, 0);
         if (item < n_heavy_items) {
           const unsigned long long kb = item * kHeavyItemChunks;
           const unsigned long long ke = min(kb + kHeavyItemChunks, hprev_tot);
           walk_chunks(I, C, Hprev, hprev_cnt, kb, ke, acc, S, lane);
+          NPS_LAP(pc, 4);
         } else {
           process_vertex_item<BS>(I, C, sm, srcq, (uint32_t)(item - n_heavy_items) * 32 + lane, srclen,
-                                  advance, T_old, want_iter, acc, S, lane);
+                                  advance, T_old, want_iter, acc, S, pc, lane);
         }
       }
     }
 
+    NPS_LAP(pc, 0);
     // ---- block tier: the CTA's warps walk the CTA list once
     __syncthreads();
     const uint32_t bcnt = min((uint32_t)(sm.blk_ctr >> 32), (uint32_t)kBlockListCap);
@@ -924,7 +1004,9 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
       __syncthreads();
       if (threadIdx.x == 0) sm.blk_ctr = 0ull;
     }
+    NPS_LAP(pc, 5);
     stage_drain(S, C, I.qcap, &ctr->status, lane);
+    NPS_LAP(pc, 6);
 
     // ---- per-CTA flush of iteration counters
     if (want_iter) {
@@ -944,19 +1026,23 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     tot.reached += acc.reached;
     tot.processed += acc.processed;
 
+    NPS_LAP(pc, 8);
     if (!team_barrier<BS>(P, sm, bar, bar_epoch, team_size, &ctr->status, false)) return;
+    NPS_LAP(pc, 7);
 
     // ---- decide the next iteration (every CTA reads the same values)
     if (advance) {
       ep += 1;
       buckets += 1;
     }
+    if (heavy_it) hg += 1;
     // thread 0 reads the shared counters once per CTA and broadcasts them
     if (threadIdx.x == 0) {
       sm.bc_q = __ldcg(&ctr->qtail[(it + 1) % 3]);
       sm.bc_h = ld_relaxed_u64(&ctr->heavy[it % 3]);
       sm.bc_f = __ldcg(&ctr->ftail[ep % 3]);
       sm.bc_m = __ldcg(&ctr->fmin[ep % 3]);
+      sm.bc_s = __ldcg(&ctr->stail[hg % 3]);
     }
     __syncthreads();
     const uint32_t qn = min(sm.bc_q, I.qcap);
@@ -994,7 +1080,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
         tr->far_len = fl;
         tr->bucket_hi = T;
         tr->delta = delta;
-        tr->level = (uint32_t)level;
+        tr->level = (uint32_t)level | (heavy_it ? 0x100u : 0u);
         for (int b = 0; b < 8; ++b) tr->hist[b] = __ldcg(&ctr->hist[sl][b]);
         tr->edges = __ldcg(&ctr->it_edges[sl]);
         tr->improvements = __ldcg(&ctr->it_impr[sl]);
@@ -1007,7 +1093,14 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     hprev_cnt = hn;
     hprev_tot = hc & kHeavyMask;
     advance = false;
-    if (qn == 0 && hn == 0) {
+    const uint32_t sn = min(sm.bc_s, I.qcap);
+    const bool split_now = I.light_heavy && delta != 0;
+    heavy_it = false;
+    if (qn == 0 && hn == 0 && split_now && sn != 0) {
+      // bucket drained: relax the heavy edges of every vertex it settled, once
+      heavy_it = true;
+      slen = sn;
+    } else if (qn == 0 && hn == 0) {
       if (fl == 0) {
         it += 1;
         break;
@@ -1035,6 +1128,12 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     atomicAdd(&ctr->improvements, (unsigned long long)r[1]);
     atomicAdd(&ctr->reached, r[2]);
     atomicAdd(&ctr->processed, (unsigned long long)r[3]);
+  }
+#ifdef NPS_PROFILE
+  if (lane == 0)
+    for (int i = 0; i < 9; ++i) atomicAdd(&ctr->prof[i], pc.acc[i]);
+#endif
+  if (threadIdx.x == 0) {
     if (rank == 0) {
       ctr->iterations = it;
       ctr->buckets = buckets;

@@ -67,6 +67,7 @@ extern "C" void nps_params_default(nps_params* p) {
   p->stream = nullptr;
   p->timeout_s = 10.0;
   p->trace = 0;
+  p->light_heavy = 1;
 }
 
 namespace {
@@ -203,8 +204,8 @@ struct nps_ctx {
   cudaStream_t stream = nullptr;
   DevInfo di;
   // per-instance workspace (single-instance calls)
-  DevBuf<int32_t> q0, q1, f0, f1;
-  DevBuf<uint32_t> mark, fmark, stamp;
+  DevBuf<int32_t> q0, q1, f0, f1, s0, s1;
+  DevBuf<uint32_t> mark, fmark, smark, stamp;
   DevBuf<int4> heavy;
   DevBuf<char> control;
   DevBuf<nps_trace_rec> trace;
@@ -247,8 +248,9 @@ nps_status ctx_init(nps_ctx* c, int device) {
 void ctx_release(nps_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  for (auto* b : {&c->q0, &c->q1, &c->f0, &c->f1, &c->g_row, &c->g_col, &c->b_pool, &c->b_order}) b->release();
-  for (auto* b : {&c->mark, &c->fmark, &c->stamp, &c->g_w, &c->g_dist, &c->b_stamp}) b->release();
+  for (auto* b : {&c->q0, &c->q1, &c->f0, &c->f1, &c->s0, &c->s1, &c->g_row, &c->g_col, &c->b_pool, &c->b_order})
+    b->release();
+  for (auto* b : {&c->mark, &c->fmark, &c->smark, &c->stamp, &c->g_w, &c->g_dist, &c->b_stamp}) b->release();
   c->heavy.release();
   c->b_heavy.release();
   c->control.release();
@@ -339,6 +341,7 @@ void fill_thresholds(const nps_params& p, InstDesc& d) {
   d.t3 = p.grid_threshold;
   d.delta = p.delta;
   d.policy = p.policy;
+  d.light_heavy = p.light_heavy != 0;
 }
 
 // Whole-launch bound: 30 per-wait timeouts, at least 60 s.
@@ -381,10 +384,11 @@ nps_status run_single(nps_ctx* c, cudaStream_t s, const int32_t* row, const int3
   const size_t nn = (size_t)n;
   nps_status e;
   if ((e = c->q0.ensure(nn, false, s)) || (e = c->q1.ensure(nn, false, s)) || (e = c->f0.ensure(nn, false, s)) ||
-      (e = c->f1.ensure(nn, false, s)))
+      (e = c->f1.ensure(nn, false, s)) || (e = c->s0.ensure(nn, false, s)) || (e = c->s1.ensure(nn, false, s)))
     return e;
   const bool grow_marks = c->mark.n < nn;
-  if ((e = c->mark.ensure(nn, true, s)) || (e = c->fmark.ensure(nn, true, s))) return e;
+  if ((e = c->mark.ensure(nn, true, s)) || (e = c->fmark.ensure(nn, true, s)) || (e = c->smark.ensure(nn, true, s)))
+    return e;
   if ((e = c->stamp.ensure(1, grow_marks || !c->stamp.p, s))) return e;
   if (grow_marks) NPS_CUDA(cudaMemsetAsync(c->stamp.p, 0, sizeof(uint32_t), s));
   const uint32_t hcap = heavy_capacity(n, m, p);
@@ -416,6 +420,9 @@ nps_status run_single(nps_ctx* c, cudaStream_t s, const int32_t* row, const int3
   d.fq[1] = c->f1.p;
   d.mark = c->mark.p;
   d.fmark = c->fmark.p;
+  d.smark = c->smark.p;
+  d.sq[0] = c->s0.p;
+  d.sq[1] = c->s1.p;
   d.heavy = c->heavy.p;
   d.qcap = (uint32_t)n;
   d.hcap = hcap;
@@ -461,6 +468,7 @@ nps_status run_single(nps_ctx* c, cudaStream_t s, const int32_t* row, const int3
 void reset_stamps(nps_ctx* c, cudaStream_t s) {
   if (c->mark.p) cudaMemsetAsync(c->mark.p, 0, c->mark.n * sizeof(uint32_t), s);
   if (c->fmark.p) cudaMemsetAsync(c->fmark.p, 0, c->fmark.n * sizeof(uint32_t), s);
+  if (c->smark.p) cudaMemsetAsync(c->smark.p, 0, c->smark.n * sizeof(uint32_t), s);
   if (c->stamp.p) cudaMemsetAsync(c->stamp.p, 0, sizeof(uint32_t), s);
   cudaStreamSynchronize(s);
 }
@@ -473,6 +481,7 @@ void fill_stats(const Counters& k, nps_stats* st) {
   st->improvements = k.improvements;
   st->vertices_processed = k.processed;
   st->status = (int32_t)k.status;
+  for (int i = 0; i < 9; ++i) st->phase_cycles[i] = k.prof[i];
 }
 
 }  // namespace
@@ -655,12 +664,12 @@ extern "C" nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, co
     size_t q_total = 0, h_total = 0;
     std::vector<uint32_t> hcap(count);
     for (int i = 0; i < count; ++i) {
-      q_total += 4 * (size_t)inst[i].n;
+      q_total += 6 * (size_t)inst[i].n;
       hcap[i] = heavy_capacity(inst[i].n, inst[i].m, p);
       h_total += hcap[i];
     }
     size_t mk_total = 0;
-    for (int i = 0; i < count; ++i) mk_total += 2 * (size_t)inst[i].n;
+    for (int i = 0; i < count; ++i) mk_total += 3 * (size_t)inst[i].n;
     if ((e = c->b_pool.ensure(q_total, false, s))) return e;
     const bool regrow = c->b_stamp.n < mk_total + (size_t)count;
     if ((e = c->b_stamp.ensure(mk_total + (size_t)count, true, s))) return e;
@@ -732,10 +741,14 @@ extern "C" nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, co
         qo += x.n;
         d.fq[k] = c->b_pool.p + qo;
         qo += x.n;
+        d.sq[k] = c->b_pool.p + qo;
+        qo += x.n;
       }
       d.mark = c->b_stamp.p + mo;
       mo += x.n;
       d.fmark = c->b_stamp.p + mo;
+      mo += x.n;
+      d.smark = c->b_stamp.p + mo;
       mo += x.n;
       d.heavy = c->b_heavy.p + ho;
       d.hcap = hcap[i];

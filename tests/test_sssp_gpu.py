@@ -46,6 +46,16 @@ def test_uniform_levels_deltas(nps, oracle, cuda_device, uniform, level, delta):
     assert st.status == 0 and st.iterations > 0
 
 
+@pytest.mark.parametrize("light_heavy", [False, True])
+@pytest.mark.parametrize("level,delta", [(1, 7), (2, 32), (3, 255), (2, 1000)])
+def test_light_heavy_split(nps, oracle, cuda_device, rmat16, grid128, light_heavy, level, delta):
+    """Heavy edges (w >= delta) relaxed once per settled vertex must give the same distances."""
+    for g in (rmat16, grid128):
+        st = _check(nps, oracle, g, g.source, _p(nps, level=level, delta=delta, light_heavy=light_heavy,
+                                                 threshold=32, block_threshold=128, grid_threshold=1024))
+        assert st.status == 0
+
+
 @pytest.mark.parametrize("bs", [128, 256, 512])
 @pytest.mark.parametrize("level", [0, 1, 2])
 def test_rmat_block_shapes(nps, oracle, cuda_device, rmat16, bs, level):
