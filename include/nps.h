@@ -200,6 +200,24 @@ nps_status nps_sssp_state(const int32_t* d_row_ptr, const int32_t* d_col, const 
  * context for `device` (at most cap records); returns the record count in *count. */
 nps_status nps_trace_read(int32_t device, nps_trace_rec* out, int32_t cap, int32_t* count);
 
+/* ---- SSSP without allocation ---------------------------------------------
+ * No counterpart in the reference.  For callers that must not allocate device
+ * memory during the call (a stream being captured in global mode, a service
+ * whose memory is all reserved in its own pool, a host that forbids allocator
+ * calls from callbacks): same result as nps_sssp with device pointers, but the
+ * kernel's workspace is a file-scope static __device__ array of
+ * NPS_NOALLOC_SCRATCH_BYTES that every GPU loading libnps holds until exit.
+ * Limit: n <= NPS_NOALLOC_MAX_VERTICES (larger graphs get NPS_ERR_CAPACITY).
+ * The first call on a device resolves the array's address (call it once before
+ * any stream capture).  Calls share the array: calls whose kernels overlap on the
+ * GPU race, so order them on one stream.  No trace, no kernel_ms in the stats.
+ * Device pointers only; p->stream selects the stream (NULL = legacy default). */
+#define NPS_NOALLOC_MAX_VERTICES 131072
+#define NPS_NOALLOC_SCRATCH_BYTES (9u << 20)
+nps_status nps_sssp_noalloc(const int32_t* d_row_ptr, const int32_t* d_col, const uint32_t* d_w,
+                            int32_t n, int64_t m, int32_t src, uint32_t* d_dist, const nps_params* p,
+                            nps_stats* st);
+
 /* ---- batched SSSP -------------------------------------------------------- */
 typedef struct nps_instance {
   const int32_t* row_ptr;  /* device pointers */

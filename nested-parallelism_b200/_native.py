@@ -97,6 +97,7 @@ SIGNATURES = {
     "nps_sssp_state": (_I32, [_P, _P, _P, _I32, _I64, _P, _P, C.POINTER(nps_params),
                               C.POINTER(nps_stats)]),
     "nps_trace_read": (_I32, [_I32, C.POINTER(nps_trace_rec), _I32, C.POINTER(_I32)]),
+    "nps_sssp_noalloc": (_I32, [_P, _P, _P, _I32, _I64, _I32, _P, C.POINTER(nps_params), C.POINTER(nps_stats)]),
     "nps_sssp_batch": (_I32, [C.POINTER(nps_instance), _I32, C.POINTER(nps_params), _I32,
                               C.POINTER(nps_stats), C.POINTER(_F)]),
     "nps_policy_set_weights": (_I32, [_I32, _P, _P, _P, _P, _P, _P]),

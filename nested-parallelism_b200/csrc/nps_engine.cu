@@ -871,3 +871,7 @@ extern "C" nps_status nps_policy_set_weights(int32_t device, const float* w1, co
   g_policy[device].set = true;
   return NPS_OK;
 }
+
+// Device copy of the learned-policy weights of `device`, or null when none were
+// loaded (used by entry points in other translation units; allocates nothing).
+const void* nps_policy_device_weights(int device) { return policy_ptr(device); }

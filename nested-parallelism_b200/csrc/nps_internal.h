@@ -14,4 +14,7 @@ void nps_clear_error();
 nps_status nps_build_csr(int32_t n, int64_t m, const int32_t* src, const int32_t* dst,
                          const uint32_t* w, bool dedupe, bool drop_self, nps_graph* out);
 
+// Device copy of the learned-policy weights of `device` (null if none loaded).
+const void* nps_policy_device_weights(int device);
+
 #endif  // NPS_INTERNAL_H_
