@@ -166,3 +166,26 @@ def timed(fn, *a, **k):
     t0 = time.perf_counter()
     r = fn(*a, **k)
     return r, time.perf_counter() - t0
+
+
+def ref_read_graph(path, fmt):
+    """The reference's readInputDIMACS9/10/SLNDC (fmt 0/1/2) + convertCSR on a file.
+    Returns (row int32[n+1], col int32[m], w uint32[m], source)."""
+    lib = _load_ref()
+    if not hasattr(lib, "_rg_typed"):
+        lib.nps_ref_read_graph.argtypes = [C.c_char_p, _I32] + [C.POINTER(_I32)] * 3 + [_P, _P, _P, _I32, _I32]
+        lib.nps_ref_read_graph.restype = C.c_int
+        lib._rg_typed = True
+    n, m, s = _I32(0), _I32(0), _I32(0)
+    p = str(path).encode()
+    rc = lib.nps_ref_read_graph(p, int(fmt), C.byref(n), C.byref(m), C.byref(s), None, None, None, 0, 0)
+    if rc != 0:
+        raise RuntimeError(f"reference reader failed ({rc})")
+    row = np.empty(n.value + 1, np.int32)
+    col = np.empty(max(m.value, 1), np.int32)
+    w = np.empty(max(m.value, 1), np.int32)
+    rc = lib.nps_ref_read_graph(p, int(fmt), C.byref(n), C.byref(m), C.byref(s), row.ctypes.data, col.ctypes.data,
+                                w.ctypes.data, n.value, m.value)
+    if rc != 0:
+        raise RuntimeError(f"reference reader failed ({rc})")
+    return row, col[: m.value], w[: m.value].view(np.uint32), int(s.value)

@@ -20,6 +20,7 @@
 #include <chrono>
 #include <cstdint>
 #include <cstdio>
+#include <cstring>
 
 #include "global.h"
 #include "heap.h"
@@ -110,6 +111,50 @@ double nps_ref_usssp_cpu(int32_t n, int32_t m, const int32_t* row, const int32_t
   usssp_cpu();
   auto t1 = std::chrono::steady_clock::now();
   return std::chrono::duration<double>(t1 - t0).count();
+}
+
+// The reference's own file front-end: readInputDIMACS9 / readInputDIMACS10 /
+// readInputSLNDC (format 0 / 1 / 2, common/global.cpp:29-190) followed by
+// convertCSR() (:192-235).  On success *n, *m, *source are set and the CSR is
+// copied into caller buffers of capacity cap_n+1 / cap_m (pass null buffers to
+// query the sizes).  Returns 0, -1 (cannot open), -2 (buffers too small).
+int nps_ref_read_graph(const char* path, int32_t format, int32_t* n, int32_t* m, int32_t* src,
+                       int32_t* row, int32_t* col, int32_t* w, int32_t cap_n, int32_t cap_m) {
+  Globals keep;
+  fp = fopen(path, "r");
+  if (!fp) return -1;
+  source = 0;
+  {
+    QuietStdout q;
+    if (format == 0) readInputDIMACS9();
+    else if (format == 1) readInputDIMACS10();
+    else readInputSLNDC();
+  }
+  fclose(fp);
+  fp = nullptr;
+  convertCSR();
+  *n = noNodeTotal;
+  *m = noEdgeTotal;
+  *src = source;
+  int rc = 0;
+  if (row && col && w) {
+    if (cap_n < noNodeTotal || cap_m < noEdgeTotal) {
+      rc = -2;
+    } else {
+      memcpy(row, graph.vertexArray, sizeof(int32_t) * (noNodeTotal + 1));
+      memcpy(col, graph.edgeArray, sizeof(int32_t) * noEdgeTotal);
+      memcpy(w, graph.weightArray, sizeof(int32_t) * noEdgeTotal);
+    }
+  }
+  delete[] graph.vertexArray;
+  delete[] graph.edgeArray;
+  delete[] graph.weightArray;
+  delete[] graph.costArray;
+  delete[] graph.levelArray;
+  delete[] graph.frontier;
+  delete[] graph.update;
+  delete[] graph.visited;
+  return rc;
 }
 
 }  // extern "C"
