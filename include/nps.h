@@ -88,7 +88,9 @@ typedef struct nps_params {
   int32_t trace;            /* 1: record one nps_trace_rec per iteration (read with nps_trace_read) */
   int32_t light_heavy;      /* 1 (default): with delta > 0, edges of weight >= delta are relaxed once,
                                when the bucket that settles their tail drains (Meyer-Sanders split) */
-  int32_t reserved[6];      /* reserved[0] = 1: test hook, the first in-kernel barrier waits for an
+  int32_t local_rounds;     /* rounds a warp spends on the vertices it just improved before taking
+                               new work (0 = none): frontiers advance several hops per barrier */
+  int32_t reserved[5];      /* reserved[0] = 1: test hook, the first in-kernel barrier waits for an
                                arrival that never comes, so its bounded wait must expire */
 } nps_params;
 

@@ -193,6 +193,7 @@ class Params:
     timeout_s: float = 10.0
     trace: bool = False
     light_heavy: bool = True            # delta > 0: heavy edges (w >= delta) relaxed once per bucket
+    local_rounds: int = 0               # warp-local rounds on just-improved vertices per work item
     fault_inject_wait: bool = False     # test hook: the first barrier can never complete
 
     def to_c(self, device_ptrs: bool, stream: Optional[int] = None) -> nps_params:
@@ -204,6 +205,7 @@ class Params:
         p.policy, p.device, p.timeout_s = self.policy, self.device, float(self.timeout_s)
         p.trace = int(bool(self.trace))
         p.light_heavy = int(bool(self.light_heavy))
+        p.local_rounds = int(self.local_rounds)
         p.device_ptrs = int(bool(device_ptrs))
         p.stream = stream
         p.reserved[0] = int(bool(self.fault_inject_wait))

@@ -34,7 +34,8 @@ class nps_params(C.Structure):
         ("grid_threshold", C.c_int32), ("block_size", C.c_int32), ("ctas_per_sm", C.c_int32),
         ("delta", C.c_uint32), ("policy", C.c_int32), ("device_ptrs", C.c_int32),
         ("device", C.c_int32), ("stream", C.c_void_p), ("timeout_s", C.c_double),
-        ("trace", C.c_int32), ("light_heavy", C.c_int32), ("reserved", C.c_int32 * 6),
+        ("trace", C.c_int32), ("light_heavy", C.c_int32), ("local_rounds", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 

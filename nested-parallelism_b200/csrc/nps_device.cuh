@@ -116,6 +116,8 @@ struct InstDesc {
   int32_t policy;
   int32_t vec_ok;       // col / w are 16-byte aligned
   int32_t light_heavy;  // 1: split edges at delta (relax w >= delta once per settled vertex)
+  int32_t local_rounds; // warp-local processing rounds per vertex item (0 = none)
+  int32_t pad1;
 };
 
 struct TeamDesc {
@@ -176,17 +178,44 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
   return v;
 }
 
-// Read-only graph streams (CSR columns and weights): no L1 allocation.
+// L2 cache policies (createpolicy, sm_80+): the CSR column/weight stream is
+// read once per scan and should leave L2 first; the per-vertex arrays touched at
+// random (distances) should stay.  Without the hint the stream (8 bytes per
+// scanned edge) evicts the distance array although both would fit in L2.
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ uint64_t policy_evict_last() {
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+
+// Read-only graph streams (CSR columns and weights): no L1 allocation, L2 evict-first.
 __device__ __forceinline__ int4 ld_stream_v4(const int32_t* p) {
   int4 v;
+#ifdef NPS_NO_L2_HINTS
   asm volatile("ld.global.nc.L1::no_allocate.v4.s32 {%0,%1,%2,%3}, [%4];"
                : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
                : "l"(p));
+#else
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0,%1,%2,%3}, [%4], %5;"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(p), "l"(policy_evict_first()));
+#endif
   return v;
 }
 __device__ __forceinline__ int32_t ld_stream(const int32_t* p) {
   int32_t v;
+#ifdef NPS_NO_L2_HINTS
   asm volatile("ld.global.nc.L1::no_allocate.s32 %0, [%1];" : "=r"(v) : "l"(p));
+#else
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;"
+               : "=r"(v)
+               : "l"(p), "l"(policy_evict_first()));
+#endif
   return v;
 }
 
@@ -203,15 +232,15 @@ __device__ __forceinline__ int deg_bin(int32_t d) {
   return b > 7 ? 7 : b;
 }
 
-// Distance read for the pre-check `nd < dist[v]` before atomicMin.  With
-// NPS_DIST_L1 the read may hit a line cached in L1 earlier in the iteration:
-// such a value can only be higher than the current one (distances only drop),
-// so a stale hit costs an atomicMin that does not improve, never a lost update.
+// Distance read for the pre-check `nd < dist[v]` before atomicMin: L2 only (the
+// value must be current), with the evict-last policy.
 __device__ __forceinline__ uint32_t ld_dist(const uint32_t* p) {
-#ifdef NPS_DIST_L1
-  return __ldca(p);
-#else
+#ifdef NPS_NO_L2_HINTS
   return __ldcg(p);
+#else
+  uint32_t v;
+  asm volatile("ld.global.cg.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(policy_evict_last()));
+  return v;
 #endif
 }
 
@@ -245,6 +274,7 @@ struct IterCtx {
   int32_t* sq;       // settle list receiving processed vertices (null: no settle appends)
   uint32_t* sq_tail;
   uint32_t sstamp;
+  int32_t local_rounds;  // rounds of warp-local processing per vertex item
 };
 
 // Whether an edge of weight w is relaxed by a pass over light (heavy = false)
@@ -596,19 +626,17 @@ __device__ __forceinline__ void warp_row(const InstDesc& I, const IterCtx& C, in
   }
 }
 
-// Vertex work item: 32 frontier entries (or far-pile entries on a bucket
-// advance), one per lane.  Warp-collective.
+// Vertex work item: up to 32 frontier entries (or far-pile entries on a bucket
+// advance), one per lane; lanes without one pass vin = -1.  Warp-collective.
 template <int BS>
 __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const IterCtx& C, Smem<BS>& sm,
-                                                    const int32_t* src_q, uint32_t idx, uint32_t src_len,
-                                                    bool advance, uint32_t T_old, bool want_hist, Acc& acc,
-                                                    Stage& S, PhaseClock& pc, int lane) {
-  int32_t v = -1, s = 0, e = 0;
+                                                    int32_t vin, bool advance, uint32_t T_old, bool want_hist,
+                                                    Acc& acc, Stage& S, PhaseClock& pc, int lane) {
+  int32_t v = vin, s = 0, e = 0;
   uint32_t du = 0;
   bool repush = false;
   int32_t rv = 0;
-  if (idx < src_len) {
-    v = src_q[idx];
+  if (v >= 0) {
     du = __ldcg(I.dist + v);
     if (advance) {
       // far-pile entry: stale below the old bound, deferred again at/above the new one
@@ -912,6 +940,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     C.sq = (C.split != 0u && !heavy_it) ? I.sq[hg & 1] : nullptr;
     C.sq_tail = &ctr->stail[hg % 3];
     C.sstamp = base + hg + 1;
+    C.local_rounds = heavy_it ? 0 : I.local_rounds;  // a heavy pass only relaxes heavy edges
     level_thresholds(level, I.t1, I.t2, I.t3, C.t_warp, C.t_block, C.t_grid);
     const int4* Hprev = I.heavy + ((it & 1) ? 0 : hhalf);
 
@@ -983,8 +1012,24 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
           walk_chunks(I, C, Hprev, hprev_cnt, kb, ke, acc, S, lane);
           NPS_LAP(pc, 4);
         } else {
-          process_vertex_item<BS>(I, C, sm, srcq, (uint32_t)(item - n_heavy_items) * 32 + lane, srclen,
-                                  advance, T_old, want_iter, acc, S, pc, lane);
+          const uint32_t idx = (uint32_t)(item - n_heavy_items) * 32 + lane;
+          process_vertex_item<BS>(I, C, sm, idx < srclen ? srcq[idx] : -1, advance, T_old, want_iter, acc, S,
+                                  pc, lane);
+          // warp-local rounds: vertices this warp just queued for the next iteration are
+          // taken back from its staging buffer and processed now, up to local_rounds times;
+          // their stamp is reset so a later improvement in this iteration queues them again
+          for (int r = 0; r < C.local_rounds && S.ncnt > 0; ++r) {
+            const uint32_t k = min(S.ncnt, 32u);
+            int32_t lv = -1;
+            if ((uint32_t)lane < k) {
+              lv = S.nbuf[S.ncnt - k + lane];
+              atomicExch(I.mark + lv, 0u);
+              __threadfence();  // the reset is visible before lv's distance is read
+            }
+            __syncwarp();
+            S.ncnt -= k;
+            process_vertex_item<BS>(I, C, sm, lv, false, T_old, want_iter, acc, S, pc, lane);
+          }
         }
       }
     }

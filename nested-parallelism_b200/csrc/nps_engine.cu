@@ -311,6 +311,7 @@ nps_status check_params(const nps_params& p) {
     return nps_fail(NPS_ERR_INVALID_ARG, "policy must be 0 (plain) or 1 (learned)");
   if (!(p.timeout_s > 0) || p.timeout_s > 3600) return nps_fail(NPS_ERR_INVALID_ARG, "timeout_s must be in (0, 3600]");
   if (p.delta >= NPS_INF) return nps_fail(NPS_ERR_INVALID_ARG, "delta must be < 2^30");
+  if (p.local_rounds < 0 || p.local_rounds > 1024) return nps_fail(NPS_ERR_INVALID_ARG, "local_rounds must be in [0, 1024]");
   return NPS_OK;
 }
 
@@ -342,6 +343,7 @@ void fill_thresholds(const nps_params& p, InstDesc& d) {
   d.delta = p.delta;
   d.policy = p.policy;
   d.light_heavy = p.light_heavy != 0;
+  d.local_rounds = p.local_rounds;
 }
 
 // Whole-launch bound: 30 per-wait timeouts, at least 60 s.

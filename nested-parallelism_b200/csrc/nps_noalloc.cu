@@ -199,6 +199,7 @@ extern "C" nps_status nps_sssp_noalloc(const int32_t* d_row_ptr, const int32_t* 
   d.delta = p.delta;
   d.policy = p.policy;
   d.light_heavy = p.light_heavy != 0;
+  d.local_rounds = p.local_rounds < 0 ? 0 : (p.local_rounds > 1024 ? 1024 : p.local_rounds);
 
   const TeamDesc td{0, grid, 0, 1};
   LaunchParams lp;

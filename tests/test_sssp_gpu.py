@@ -263,3 +263,13 @@ def test_invalid_arguments(nps, cuda_device, uniform):
         assert ei.value.status == 1
     with pytest.raises(nps.NpsError):
         nps.sssp(uniform, uniform.n)  # source out of range
+
+
+@pytest.mark.parametrize("rounds", [1, 3, 16])
+@pytest.mark.parametrize("level,delta,lh", [(2, 0, False), (3, 40, True), (1, 300, False), (0, 16, True)])
+def test_warp_local_rounds(nps, oracle, cuda_device, rmat16, grid128, rounds, level, delta, lh):
+    """Vertices a warp improves are processed by that warp within the same
+    iteration for up to `rounds` rounds; distances must not change."""
+    for g in (rmat16, grid128):
+        _check(nps, oracle, g, g.source, _p(nps, level=level, delta=delta, light_heavy=lh, local_rounds=rounds,
+                                           threshold=32, block_threshold=128, grid_threshold=1024))
