@@ -129,6 +129,7 @@ typedef struct nps_trace_rec {
   uint32_t reached;         /* vertices reached so far */
   uint32_t heavy;           /* grid-tier rows collected for the next iteration */
   uint64_t t_ns;            /* device time since the launch began, at the end of the iteration */
+  float feat[12];           /* the learned policy's input features after this iteration (raw) */
 } nps_trace_rec;
 
 /* Host-side CSR graph, library-allocated; free with nps_graph_free. */

@@ -347,5 +347,5 @@ def trace_read(device: int = 0, cap: int = 1 << 16) -> List[dict]:
         out.append(dict(iteration=r.iteration, frontier=r.frontier, far_len=r.far_len,
                         bucket_hi=r.bucket_hi, delta=r.delta, level=r.level, hist=list(r.hist),
                         edges=int(r.edges), improvements=int(r.improvements), reached=r.reached,
-                        heavy=r.heavy, t_us=r.t_ns / 1e3))
+                        heavy=r.heavy, t_us=r.t_ns / 1e3, feat=list(r.feat)))
     return out

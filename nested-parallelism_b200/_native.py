@@ -55,6 +55,7 @@ class nps_trace_rec(C.Structure):
         ("bucket_hi", C.c_uint32), ("delta", C.c_uint32), ("level", C.c_uint32),
         ("hist", C.c_uint32 * 8), ("edges", C.c_uint64), ("improvements", C.c_uint64),
         ("reached", C.c_uint32), ("heavy", C.c_uint32), ("t_ns", C.c_uint64),
+        ("feat", C.c_float * 12),
     ]
 
 

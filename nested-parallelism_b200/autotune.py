@@ -1,0 +1,183 @@
+"""Autotuner for the persistent SSSP kernel's parameters.
+
+Picks the consolidation level and degree thresholds, the block shape (threads
+per CTA, CTAs per SM), the bucket width delta, the light/heavy split and the
+warp-local rounds for a class of graphs by timing the CUDA kernel itself on
+sample graphs (device-resident, CUDA-event kernel times, median of repeats).
+
+Search: coordinate descent over a discrete space.  Starting from a seed
+configuration, each parameter in turn is set to every value of its axis with
+the others held; the best is kept; passes repeat until a pass changes nothing
+or the evaluation budget is spent.  Every configuration gives the same exact
+distances (delta stepping and every consolidation level are exact), which the
+tuner checks against the seed run.
+
+The reference fixes THRESHOLD = 64 and CONSOLIDATE_LEVEL at compile time
+(apps/sssp/src/gpu/sssp_kernel.cu:7, sssp_wrapper.cu:14-16); here they are
+runtime parameters and this module chooses them.
+"""
+from __future__ import annotations
+
+import dataclasses
+import json
+import os
+import statistics
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import Params, sssp_batch, sssp_device
+
+AXES: Dict[str, List] = {
+    "level": [0, 1, 2, 3],
+    "threshold": [16, 32, 64, 128],
+    "grid_threshold": [512, 2048, 8192],
+    "block_size": [256, 512],
+    "ctas_per_sm": [0, 1],
+    "delta": [0, 8, 16, 32, 64, 128, 256, 1024, 4096, 16384, 65536],
+    "light_heavy": [False, True],
+    "local_rounds": [0, 2, 8],
+}
+ORDER = ["delta", "level", "threshold", "light_heavy", "grid_threshold", "block_size", "local_rounds",
+         "ctas_per_sm"]
+
+
+@dataclasses.dataclass
+class DeviceGraph:
+    """A graph already on the device (tensors or raw pointers)."""
+    row_ptr: object
+    col: object
+    w: object
+    dist: object
+    n: int
+    m: int
+    src: int
+
+
+def to_device(g, src: Optional[int] = None, device=None) -> DeviceGraph:
+    """Copy a host Graph to device tensors (torch is used for device memory only)."""
+    import torch
+    dev = device or torch.device("cuda", 0)
+
+    def t(a):
+        return torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).to(dev)
+
+    return DeviceGraph(t(g.row_ptr), t(g.col), t(g.w), torch.empty(g.n, dtype=torch.int32, device=dev), g.n, g.m,
+                       g.source if src is None else int(src))
+
+
+def _key(p: Params) -> Tuple:
+    return tuple(sorted(dataclasses.asdict(p).items()))
+
+
+def _normalise(p: Params) -> Params:
+    # keep the hybrid thresholds ordered; block_threshold sits between threshold and grid_threshold
+    q = dataclasses.replace(p)
+    if q.grid_threshold < q.threshold:
+        q.grid_threshold = q.threshold
+    q.block_threshold = int(min(max(q.threshold, round((q.threshold * q.grid_threshold) ** 0.5)), q.grid_threshold))
+    return q
+
+
+class Autotuner:
+    def __init__(self, graphs: Sequence[DeviceGraph], repeats: int = 3, budget: int = 80,
+                 axes: Optional[Dict[str, List]] = None, batch: bool = False, verbose: bool = False):
+        self.graphs = list(graphs)
+        self.repeats = repeats
+        self.budget = budget
+        self.axes = dict(AXES if axes is None else axes)
+        self.batch = batch
+        self.verbose = verbose
+        self.cache: Dict[Tuple, float] = {}
+        self.reference = None
+        self.log: List[dict] = []
+
+    def _time_once(self, p: Params) -> float:
+        import torch
+        if self.batch:
+            from . import Instance
+            inst = [Instance(g.row_ptr, g.col, g.w, g.dist, g.n, g.m, g.src) for g in self.graphs]
+            _, ms = sssp_batch(inst, p, use_graph=False)
+            torch.cuda.synchronize()
+            return ms
+        total = 0.0
+        for g in self.graphs:
+            st = sssp_device(g.row_ptr, g.col, g.w, g.n, g.m, g.src, g.dist, p)
+            total += st.kernel_ms
+        torch.cuda.synchronize()
+        return total
+
+    def _distances(self):
+        return [g.dist.cpu().numpy().copy() for g in self.graphs]
+
+    def evaluate(self, p: Params) -> float:
+        p = _normalise(p)
+        k = _key(p)
+        if k in self.cache:
+            return self.cache[k]
+        self._time_once(p)  # warm-up (workspace growth, caches)
+        times = [self._time_once(p) for _ in range(self.repeats)]
+        ms = statistics.median(times)
+        d = self._distances()
+        if self.reference is None:
+            self.reference = d
+        elif not all(np.array_equal(a, b) for a, b in zip(d, self.reference)):
+            raise AssertionError(f"configuration {p} changed the distances")
+        self.cache[k] = ms
+        self.log.append({"params": dataclasses.asdict(p), "ms": ms})
+        if self.verbose:
+            print(f"  {ms:9.3f} ms  {dataclasses.asdict(p)}", flush=True)
+        return ms
+
+    def run(self, seed: Optional[Params] = None) -> Tuple[Params, float]:
+        best = _normalise(seed or Params(level=2, threshold=64, delta=0, block_size=512))
+        best_ms = self.evaluate(best)
+        changed = True
+        while changed and len(self.cache) < self.budget:
+            changed = False
+            for name in ORDER:
+                if name not in self.axes:
+                    continue
+                for val in self.axes[name]:
+                    if len(self.cache) >= self.budget:
+                        break
+                    if getattr(best, name) == val:
+                        continue
+                    if name == "grid_threshold" and best.level != 3:
+                        continue  # only the hybrid level uses it
+                    if name == "light_heavy" and best.delta == 0:
+                        continue
+                    cand = _normalise(dataclasses.replace(best, **{name: val}))
+                    ms = self.evaluate(cand)
+                    if ms < best_ms * 0.995:
+                        best, best_ms, changed = cand, ms, True
+        return best, best_ms
+
+
+def autotune(graphs: Sequence[DeviceGraph], repeats: int = 3, budget: int = 80, seed: Optional[Params] = None,
+             axes: Optional[Dict[str, List]] = None, batch: bool = False, verbose: bool = False):
+    """Tune Params for these device-resident graphs; returns (Params, ms, log)."""
+    t = Autotuner(graphs, repeats=repeats, budget=budget, axes=axes, batch=batch, verbose=verbose)
+    p, ms = t.run(seed)
+    return p, ms, t.log
+
+
+def save(path: str, key: str, p: Params, ms: float) -> None:
+    """Record a tuned configuration under `key` (a graph-class name) in a JSON file."""
+    data = {}
+    if os.path.exists(path):
+        with open(path) as f:
+            data = json.load(f)
+    data[key] = {"params": dataclasses.asdict(p), "ms": ms}
+    with open(path, "w") as f:
+        json.dump(data, f, indent=1, sort_keys=True)
+
+
+def load(path: str, key: str) -> Optional[Params]:
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        data = json.load(f)
+    if key not in data:
+        return None
+    return Params(**data[key]["params"])

@@ -1099,39 +1099,44 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     if (want_iter) {
       const uint32_t sl = it % 3;
       reached_total += __ldcg(&ctr->it_reached[sl]);
-      if (learned) {
-        // 12 features: log2 next frontier, 8 degree-histogram fractions of this
-        // iteration's frontier, log2 bucket index, reached fraction, improvements per edge
-        if (threadIdx.x == 0) {
-          float h[8], hs = 0.f;
-          for (int b = 0; b < 8; ++b) { h[b] = (float)__ldcg(&ctr->hist[sl][b]); hs += h[b]; }
-          const float inv = hs > 0.f ? 1.f / hs : 0.f;
-          float f[NPS_MLP_IN];
-          f[0] = log2f(1.f + (float)(will_advance ? fl : qn));
-          for (int b = 0; b < 8; ++b) f[1 + b] = h[b] * inv;
-          f[9] = log2f(1.f + (float)buckets);
-          f[10] = (float)reached_total / (float)I.n;
-          const unsigned long long ie = __ldcg(&ctr->it_edges[sl]);
-          f[11] = ie ? (float)__ldcg(&ctr->it_impr[sl]) / (float)ie : 0.f;
+      const int level_used = level;
+      // The 12 policy features, computed by thread 0 of every CTA from the same
+      // counters (so every CTA takes the same decision): log2 of the next frontier,
+      // the out-degree histogram of this iteration's frontier as 8 fractions,
+      // log2(1 + bucket advances), the reached fraction, improvements per scanned edge.
+      if (threadIdx.x == 0) {
+        float h[8], hs = 0.f;
+        for (int b = 0; b < 8; ++b) { h[b] = (float)__ldcg(&ctr->hist[sl][b]); hs += h[b]; }
+        const float inv = hs > 0.f ? 1.f / hs : 0.f;
+        float f[NPS_MLP_IN];
+        f[0] = log2f(1.f + (float)(will_advance ? fl : qn));
+        for (int b = 0; b < 8; ++b) f[1 + b] = h[b] * inv;
+        f[9] = log2f(1.f + (float)buckets);
+        f[10] = (float)reached_total / (float)I.n;
+        const unsigned long long ie = __ldcg(&ctr->it_edges[sl]);
+        f[11] = ie ? (float)__ldcg(&ctr->it_impr[sl]) / (float)ie : 0.f;
+        if (learned)
           for (int i = 0; i < NPS_MLP_IN; ++i) sm.feat[i] = (f[i] - P.policy->mean[i]) * P.policy->istd[i];
+        if (I.trace && rank == 0 && it < I.trace_cap) {
+          nps_trace_rec* tr = I.trace + it;
+          tr->iteration = it;
+          tr->frontier = srclen;
+          tr->far_len = fl;
+          tr->bucket_hi = T;
+          tr->delta = delta;
+          tr->level = (uint32_t)level_used | (heavy_it ? 0x100u : 0u) | (advance ? 0x200u : 0u);
+          for (int b = 0; b < 8; ++b) tr->hist[b] = __ldcg(&ctr->hist[sl][b]);
+          tr->edges = ie;
+          tr->improvements = __ldcg(&ctr->it_impr[sl]);
+          tr->reached = reached_total;
+          tr->heavy = hn;
+          tr->t_ns = globaltimer_ns() - sm.t_start;
+          for (int i = 0; i < NPS_MLP_IN; ++i) tr->feat[i] = f[i];
         }
+      }
+      if (learned) {
         policy_eval<BS>(P.policy, sm);
         level = sm.pol_choice[1];
-      }
-      if (I.trace && rank == 0 && threadIdx.x == 0 && it < I.trace_cap) {
-        nps_trace_rec* tr = I.trace + it;
-        tr->iteration = it;
-        tr->frontier = srclen;
-        tr->far_len = fl;
-        tr->bucket_hi = T;
-        tr->delta = delta;
-        tr->level = (uint32_t)level | (heavy_it ? 0x100u : 0u);
-        for (int b = 0; b < 8; ++b) tr->hist[b] = __ldcg(&ctr->hist[sl][b]);
-        tr->edges = __ldcg(&ctr->it_edges[sl]);
-        tr->improvements = __ldcg(&ctr->it_impr[sl]);
-        tr->reached = reached_total;
-        tr->heavy = hn;
-        tr->t_ns = globaltimer_ns() - sm.t_start;
       }
     }
 

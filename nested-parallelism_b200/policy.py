@@ -157,3 +157,108 @@ def smoke_step(device) -> float:
     tr.torch.cuda.synchronize(device)
     assert np.isfinite(loss) and loss > 0
     return loss
+
+
+# ---------------------------------------------------------------------------
+# Training data from traces of plain runs.
+#
+# For every training graph the plain kernel runs once per fixed configuration
+# (delta in DELTA_CHOICES x level in LEVEL_CHOICES, the other parameters those
+# of the plain autotuned configuration) with tracing on.  A trace record holds
+# the kernel's own feature vector after an iteration and the device time at
+# which the iteration ended.  Each record is placed in a progress bin (reached
+# vertices at that point over the reached total); the cost of a configuration
+# in a bin is the device time of the iterations that start in it.  Every record
+# of a graph is labelled with the configuration that is cheapest in the
+# record's bin, weighted by how much that choice saves there against the median
+# configuration.  The network so learns which bucket width and consolidation
+# level pay off in which phase of a run.
+
+DELTA_CHOICES = [1 << k for k in range(11)]
+LEVEL_CHOICES = [0, 1, 2]
+PROGRESS_BINS = np.array([0.0, 1e-3, 1e-2, 0.05, 0.2, 0.5, 0.8, 0.95, 0.99, 1.01])
+
+
+def trace_run(dg, params, device: int = 0):
+    """One traced run on a device-resident graph; returns (kernel_ms, records)."""
+    import dataclasses as _dc
+    from . import sssp_device, trace_read
+    p = _dc.replace(params, trace=True, policy=0)
+    st = sssp_device(dg.row_ptr, dg.col, dg.w, dg.n, dg.m, dg.src, dg.dist, p)
+    return st.kernel_ms, trace_read(device)
+
+
+def config_params(base, delta: int, level: int):
+    import dataclasses as _dc
+    return _dc.replace(base, delta=delta, level=level)
+
+
+def _spread(c, p0, p1, dt):
+    """Add an iteration's time dt to the progress bins its span [p0, p1) overlaps,
+    in proportion to the overlap; a span without progress charges its own bin."""
+    nb = len(PROGRESS_BINS) - 1
+    if p1 <= p0 + 1e-12:
+        b = int(np.searchsorted(PROGRESS_BINS, p0, side="right") - 1)
+        c[min(max(b, 0), nb - 1)] += dt
+        return
+    lo = np.maximum(PROGRESS_BINS[:-1], p0)
+    hi = np.minimum(PROGRESS_BINS[1:], p1)
+    c += dt * np.clip(hi - lo, 0.0, None) / (p1 - p0)
+
+
+def label_graph(runs):
+    """runs: {(delta_idx, level_idx): (ms, records)} for one graph.
+    Returns X [R, 12], yd [R], yl [R], wt [R] over all records of all runs."""
+    final = max(recs[-1]["reached"] for _, recs in runs.values() if recs)
+    nb = len(PROGRESS_BINS) - 1
+    cost = {}
+    rows = []
+    for cfg, (ms, recs) in runs.items():
+        c = np.zeros(nb)
+        prev_t = 0.0
+        prev_p = 0.0
+        for r in recs:
+            p1 = r["reached"] / max(final, 1)
+            _spread(c, prev_p, p1, r["t_us"] - prev_t)
+            prev_t = r["t_us"]
+            prev_p = p1
+            # the decision taken after this record shapes the iterations that start here
+            b = min(max(int(np.searchsorted(PROGRESS_BINS, p1, side="right") - 1), 0), nb - 1)
+            rows.append((cfg, b, r["feat"]))
+        cost[cfg] = c
+    cfgs = list(cost)
+    C = np.stack([cost[k] for k in cfgs])  # [configs, bins]
+    best = C.argmin(axis=0)
+    gain = np.median(C, axis=0) - C.min(axis=0)
+    X, yd, yl, wt = [], [], [], []
+    for cfg, b, feat in rows:
+        d_i, l_i = cfgs[best[b]]
+        X.append(feat)
+        yd.append(d_i)
+        yl.append(l_i)
+        wt.append(gain[b] + 1e-3)
+    return (np.array(X, np.float32), np.array(yd, np.int64), np.array(yl, np.int64), np.array(wt, np.float32))
+
+
+def train(X, yd, yl, wt, device, steps: int = 1500, lr: float = 3e-3, seed: int = 0, log_every: int = 0):
+    """Fit the policy on the GPU with the library's kernels; returns (MLPWeights, losses)."""
+    mean = X.mean(axis=0).astype(np.float32)
+    std = X.std(axis=0).astype(np.float32)
+    istd = np.where(std > 1e-6, 1.0 / np.maximum(std, 1e-6), 0.0).astype(np.float32)
+    Xn = ((X - mean) * istd).astype(np.float32)
+    w = MLPWeights.init(seed)
+    w.mean, w.istd = mean, istd
+    tr = GPUTrainer(w, device, lr=lr)
+    t = tr.torch
+    Xd = t.as_tensor(Xn, device=device)
+    ydd = t.as_tensor(yd.astype(np.int32), device=device)
+    yld = t.as_tensor(yl.astype(np.int32), device=device)
+    wtd = t.as_tensor(wt / wt.mean(), device=device)
+    losses = []
+    for i in range(steps):
+        loss = tr.loss_backward(Xd, ydd, yld, wtd)
+        tr.adam_step()
+        if log_every and i % log_every == 0:
+            losses.append(float(loss.item()))
+    losses.append(float(tr.loss_backward(Xd, ydd, yld, wtd).item()))
+    return tr.weights(), losses
