@@ -531,16 +531,17 @@ struct Smem {
 // (setting NPS_ERR_TIMEOUT and the abort flag) or when the abort flag is set.
 // Returns false when the computation must stop.
 //
-// Two-level arrival: the CTAs of each group of kBarGroup count in on their
-// group's word; the last of a group counts the group in on the root word; the
-// last group publishes the new generation, which every CTA polls.  Words are
-// 128 bytes apart: bar[0] root, bar[32] generation, bar[64 + 32 g] group g.
-constexpr uint32_t kBarGroup = 16;
+// Arrival is one `red.release.gpu` add per CTA on the team's counter (release:
+// the CTA's writes, made thread 0's by the preceding bar.sync, become visible
+// with the arrival); thread 0 then polls the counter with `ld.acquire.gpu` until
+// it reaches epoch * team_size.  With check_status = false the caller reads the
+// status word itself, together with the counters it needs after the barrier.
+constexpr uint32_t kBarGroup = 16;  // barrier-area sizing granule (words per team = 32 * (2 + CTAs / 16))
 
 template <int BS>
 __device__ __forceinline__ bool team_barrier(const LaunchParams& P, Smem<BS>& sm, uint32_t* bar,
                                              uint32_t& epoch, uint32_t team_size,
-                                             uint32_t* status, bool inject) {
+                                             uint32_t* status, bool inject, bool check_status = true) {
   __syncthreads();
   if (threadIdx.x == 0) {
     if (globaltimer_ns() - sm.t_start > P.run_budget_ns) {
@@ -548,34 +549,24 @@ __device__ __forceinline__ bool team_barrier(const LaunchParams& P, Smem<BS>& sm
       atomicExch(P.abort_flag, 1u);
     }
     epoch += 1;
-    const uint32_t rank = sm.rank;
-    const uint32_t g = rank / kBarGroup;
-    const uint32_t gsz = min(kBarGroup, team_size - g * kBarGroup);
-    const uint32_t ngroups = (team_size + kBarGroup - 1) / kBarGroup;
-    __threadfence();
-    if (atomicAdd(bar + 64 + 32 * g, 1u) == epoch * gsz - 1) {
-      __threadfence();
-      if (atomicAdd(bar, 1u) == epoch * ngroups - 1) {
-        __threadfence();
-        atomicExch(bar + 32, epoch);
-      }
-    }
-    const uint32_t target = epoch + (inject ? 1u : 0u);
-    unsigned long long t0 = globaltimer_ns();
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
+    const uint32_t target = epoch * team_size + (inject ? 1u : 0u);
+    const unsigned long long t0 = globaltimer_ns();
     int ok = 1;
     uint32_t spins = 0;
-    while ((int32_t)(ld_acquire_u32(bar + 32) - target) < 0) {
-      if (ld_relaxed_u32(P.abort_flag)) { ok = 0; break; }
-      if ((++spins & 15u) == 0 && globaltimer_ns() - t0 > P.timeout_ns) {
-        atomicCAS(status, 0u, (uint32_t)NPS_ERR_TIMEOUT);
-        atomicExch(P.abort_flag, 1u);
-        ok = 0;
-        break;
+    while ((int32_t)(ld_acquire_u32(bar) - target) < 0) {
+      if ((++spins & 15u) == 0) {
+        if (ld_relaxed_u32(P.abort_flag)) { ok = 0; break; }
+        if (globaltimer_ns() - t0 > P.timeout_ns) {
+          atomicCAS(status, 0u, (uint32_t)NPS_ERR_TIMEOUT);
+          atomicExch(P.abort_flag, 1u);
+          ok = 0;
+          break;
+        }
       }
       __nanosleep(20);
     }
-    __threadfence();
-    if (ok && ld_relaxed_u32(status) != 0) ok = 0;
+    if (ok && check_status && ld_relaxed_u32(status) != 0) ok = 0;
     if (!ok) atomicExch(P.abort_flag, 1u);
     sm.ok = ok;
   }
@@ -977,34 +968,44 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     S.fcnt = 0;
     S.scnt = 0;
 
-    // ---- warp work loop over striped counters: heavy chunk items, then vertex items.
-    // Warps beyond four per item stay out; an exhausted stripe is recognised by a
-    // plain read before any atomic is spent on it.
-    // The next item's index is requested before the current item is processed,
-    // so the atomic's round trip overlaps the work.
-    if ((unsigned long long)gwarp < 4ull * n_items + kStripes) {
+    // ---- work loop: heavy chunk items, then vertex items.  With no more items than
+    // warps, warp w takes item w (no atomics); otherwise items come from striped
+    // counters, the next index requested before the current item is processed, and
+    // an exhausted stripe answered by a parallel probe of all stripes.
+    {
+      const uint32_t team_warps = team_size * NW;
+      const bool static_items = n_items <= team_warps;
       uint32_t* wc = &ctr->work[it % 3][0];
       int stripe = (int)(gwarp % kStripes);
-      uint32_t t_next = 0xffffffffu;
+      uint32_t t_next = 0;
       bool have_next = false;
-      for (int tried = 0; tried < kStripes;) {
-        const uint32_t stripe_items = n_items > (uint32_t)stripe ? (n_items - stripe + kStripes - 1) / kStripes : 0u;
-        uint32_t t = 0xffffffffu;
-        if (have_next) {
-          t = t_next;
-        } else if (lane == 0 && ld_relaxed_u32(&wc[stripe * 32]) < stripe_items) {
-          t = atomicAdd(&wc[stripe * 32], 1u);
+      bool static_done = false;
+      for (;;) {
+        unsigned long long item;
+        if (static_items) {
+          if (static_done || gwarp >= n_items) break;
+          static_done = true;
+          item = gwarp;
+        } else {
+          uint32_t t = 0;
+          if (lane == 0) t = have_next ? t_next : atomicAdd(&wc[stripe * 32], 1u);
+          t = __shfl_sync(kFull, t, 0);
+          have_next = false;
+          const uint32_t my_items = n_items > (uint32_t)stripe ? (n_items - stripe + kStripes - 1) / kStripes : 0u;
+          if (t >= my_items) {
+            // probe every stripe at once; continue on the first one with items left
+            const uint32_t li = n_items > (uint32_t)lane ? (n_items - lane + kStripes - 1) / kStripes : 0u;
+            const bool avail = lane < kStripes && ld_relaxed_u32(&wc[lane * 32]) < li;
+            const uint32_t m = __ballot_sync(kFull, avail);
+            if (m == 0) break;
+            const uint32_t rot = ((m >> (stripe + 1)) | (m << (kStripes - stripe - 1))) & ((1u << kStripes) - 1);
+            stripe = (stripe + __ffs(rot)) % kStripes;
+            continue;
+          }
+          if (lane == 0) t_next = atomicAdd(&wc[stripe * 32], 1u);
+          have_next = true;
+          item = (unsigned long long)t * kStripes + stripe;
         }
-        t = __shfl_sync(kFull, t, 0);
-        have_next = false;
-        if (t >= stripe_items) {
-          stripe = (stripe + 1) % kStripes;
-          ++tried;
-          continue;
-        }
-        if (lane == 0) t_next = atomicAdd(&wc[stripe * 32], 1u);
-        have_next = true;
-        const unsigned long long item = (unsigned long long)t * kStripes + stripe;
         NPS_LAP(pc, 0);
         if (item < n_heavy_items) {
           const unsigned long long kb = item * kHeavyItemChunks;
@@ -1033,7 +1034,6 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
         }
       }
     }
-
     NPS_LAP(pc, 0);
     // ---- block tier: the CTA's warps walk the CTA list once
     __syncthreads();
@@ -1072,7 +1072,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     tot.processed += acc.processed;
 
     NPS_LAP(pc, 8);
-    if (!team_barrier<BS>(P, sm, bar, bar_epoch, team_size, &ctr->status, false)) return;
+    if (!team_barrier<BS>(P, sm, bar, bar_epoch, team_size, &ctr->status, false, false)) return;
     NPS_LAP(pc, 7);
 
     // ---- decide the next iteration (every CTA reads the same values)
@@ -1081,15 +1081,20 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
       buckets += 1;
     }
     if (heavy_it) hg += 1;
-    // thread 0 reads the shared counters once per CTA and broadcasts them
+    // thread 0 reads the shared counters and the status word once per CTA and broadcasts them
     if (threadIdx.x == 0) {
       sm.bc_q = __ldcg(&ctr->qtail[(it + 1) % 3]);
       sm.bc_h = ld_relaxed_u64(&ctr->heavy[it % 3]);
       sm.bc_f = __ldcg(&ctr->ftail[ep % 3]);
       sm.bc_m = __ldcg(&ctr->fmin[ep % 3]);
       sm.bc_s = __ldcg(&ctr->stail[hg % 3]);
+      if (ld_relaxed_u32(&ctr->status) != 0) {
+        atomicExch(P.abort_flag, 1u);
+        sm.ok = 0;
+      }
     }
     __syncthreads();
+    if (!sm.ok) return;
     const uint32_t qn = min(sm.bc_q, I.qcap);
     const unsigned long long hc = sm.bc_h;
     const uint32_t hn = min((uint32_t)(hc >> kHeavyShift), hhalf);
