@@ -90,7 +90,10 @@ typedef struct nps_params {
                                when the bucket that settles their tail drains (Meyer-Sanders split) */
   int32_t local_rounds;     /* rounds a warp spends on the vertices it just improved before taking
                                new work (0 = none): frontiers advance several hops per barrier */
-  int32_t reserved[5];      /* reserved[0] = 1: test hook, the first in-kernel barrier waits for an
+  int32_t order_degree;     /* with delta > 0: an improved vertex whose out-degree is below this
+                               joins the current bucket whatever its distance, so only rows of at
+                               least this degree wait for their bucket (0 = every vertex waits) */
+  int32_t reserved[4];      /* reserved[0] = 1: test hook, the first in-kernel barrier waits for an
                                arrival that never comes, so its bounded wait must expire */
 } nps_params;
 
@@ -216,7 +219,7 @@ nps_status nps_trace_read(int32_t device, nps_trace_rec* out, int32_t cap, int32
  * GPU race, so order them on one stream.  No trace, no kernel_ms in the stats.
  * Device pointers only; p->stream selects the stream (NULL = legacy default). */
 #define NPS_NOALLOC_MAX_VERTICES 131072
-#define NPS_NOALLOC_SCRATCH_BYTES (9u << 20)
+#define NPS_NOALLOC_SCRATCH_BYTES (10u << 20)
 nps_status nps_sssp_noalloc(const int32_t* d_row_ptr, const int32_t* d_col, const uint32_t* d_w,
                             int32_t n, int64_t m, int32_t src, uint32_t* d_dist, const nps_params* p,
                             nps_stats* st);

@@ -194,6 +194,7 @@ class Params:
     trace: bool = False
     light_heavy: bool = True            # delta > 0: heavy edges (w >= delta) relaxed once per bucket
     local_rounds: int = 0               # warp-local rounds on just-improved vertices per work item
+    order_degree: int = 0               # delta > 0: rows below this degree ignore the bucket bound
     fault_inject_wait: bool = False     # test hook: the first barrier can never complete
 
     def to_c(self, device_ptrs: bool, stream: Optional[int] = None) -> nps_params:
@@ -206,6 +207,7 @@ class Params:
         p.trace = int(bool(self.trace))
         p.light_heavy = int(bool(self.light_heavy))
         p.local_rounds = int(self.local_rounds)
+        p.order_degree = int(self.order_degree)
         p.device_ptrs = int(bool(device_ptrs))
         p.stream = stream
         p.reserved[0] = int(bool(self.fault_inject_wait))

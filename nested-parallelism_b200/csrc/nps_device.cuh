@@ -57,7 +57,7 @@ constexpr uint32_t kInf = NPS_INF;
 constexpr int kHeavyShift = 36;  // heavy counter packs (count << 36) | chunk_offset
 constexpr unsigned long long kHeavyMask = (1ull << kHeavyShift) - 1;
 constexpr int kStripes = 8;            // striped work counters
-constexpr int kHeavyItemChunks = 64;   // chunks (4 edges each) per heavy work item
+constexpr int kHeavyItemShift = 6;     // at least 2^6 chunks (256 edges) per grid-tier work item
 constexpr int kBlockListCap = 512;     // CTA list entries (block tier)
 
 // Per-instance device counters.  Zeroed by the host before a launch.
@@ -102,6 +102,9 @@ struct InstDesc {
   uint32_t* mark;       // near-queue dedupe stamps
   uint32_t* fmark;      // far-pile dedupe stamps
   int4* heavy;          // grid-tier entries {row start, row end, vertex | heavy flag, chunk offset}
+  int32_t* hitem;       // per half: entry holding the first chunk of each grid-tier work item
+  uint32_t icap;        // work items per half
+  uint32_t item_shift;  // log2 chunks per grid-tier work item (>= kHeavyItemShift)
   int32_t* sq[2];       // settle lists (light/heavy split): vertices processed in the bucket
   uint32_t* smark;      // settle-list dedupe stamps
   uint32_t qcap;
@@ -117,7 +120,7 @@ struct InstDesc {
   int32_t vec_ok;       // col / w are 16-byte aligned
   int32_t light_heavy;  // 1: split edges at delta (relax w >= delta once per settled vertex)
   int32_t local_rounds; // warp-local processing rounds per vertex item (0 = none)
-  int32_t pad1;
+  int32_t order_degree; // rows below this degree ignore the bucket bound (0 = none)
 };
 
 struct TeamDesc {
@@ -235,7 +238,11 @@ __device__ __forceinline__ int deg_bin(int32_t d) {
 // Distance read for the pre-check `nd < dist[v]` before atomicMin: L2 only (the
 // value must be current), with the evict-last policy.
 __device__ __forceinline__ uint32_t ld_dist(const uint32_t* p) {
-#ifdef NPS_NO_L2_HINTS
+#if defined(NPS_DIST_L1)
+  uint32_t v;
+  asm volatile("ld.global.ca.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(policy_evict_last()));
+  return v;
+#elif defined(NPS_NO_L2_HINTS)
   return __ldcg(p);
 #else
   uint32_t v;
@@ -266,6 +273,7 @@ struct IterCtx {
   int4* heavy;       // grid-tier list receiving appends
   unsigned long long* heavy_ctr;
   uint32_t hcap;     // capacity of that list
+  int32_t* hitem;    // its work-item start entries
   int32_t t_warp;    // degree >= t_warp leaves the small path
   int32_t t_block;   // degree >= t_block goes to the CTA list
   int32_t t_grid;    // degree >= t_grid goes to H
@@ -275,6 +283,7 @@ struct IterCtx {
   uint32_t* sq_tail;
   uint32_t sstamp;
   int32_t local_rounds;  // rounds of warp-local processing per vertex item
+  int32_t order_deg;     // improved vertices below this degree join the near queue at any distance
 };
 
 // Whether an edge of weight w is relaxed by a pass over light (heavy = false)
@@ -356,7 +365,9 @@ __device__ __forceinline__ void relax_batch(const InstDesc& I, const IterCtx& C,
       acc.impr++;
       if (old[j] == kInf) acc.reached++;
       // one exchange decides whether this improvement is the first of the iteration
-      if (nd[j] < C.T) {
+      bool near = nd[j] < C.T;
+      if (!near && C.order_deg > 0) near = __ldg(I.row_ptr + v[j] + 1) - __ldg(I.row_ptr + v[j]) < C.order_deg;
+      if (near) {
         pn[j] = atomicExch(I.mark + v[j], C.snear) != C.snear;
       } else {
         pf[j] = atomicExch(I.fmark + v[j], C.sfar) != C.sfar;
@@ -667,6 +678,7 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
     stage_k<1>(S.sbuf, S.scnt, f, vv, C.sq, C.sq_tail, I.qcap, &I.ctr->status, lane);
   }
   // deferred entries remember which edges they relax in the top bit of the vertex id
+  // deferred entries remember which edges they relax in the top bit of the vertex id
   const int32_t vtag = C.heavy_iter ? (int32_t)((uint32_t)v | 0x80000000u) : v;
   const bool small = deg > 0 && deg < C.t_warp;
   bool wtier = deg >= C.t_warp && deg < C.t_block;
@@ -683,8 +695,18 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
     const uint32_t nch = row_chunks(s, e);
     const unsigned long long old = atomicAdd(C.heavy_ctr, (1ull << kHeavyShift) | nch);
     const uint32_t slot = (uint32_t)(old >> kHeavyShift);
-    if (slot < C.hcap) C.heavy[slot] = make_int4(s, e, vtag, (int32_t)(uint32_t)(old & kHeavyMask));
-    else atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_CAPACITY);
+    const uint32_t off = (uint32_t)(old & kHeavyMask);
+    if (slot < C.hcap) {
+      C.heavy[slot] = make_int4(s, e, vtag, (int32_t)off);
+      // this entry holds the first chunk of every work item that starts inside it
+      const uint32_t sh = I.item_shift;
+      for (uint32_t b = (off + (1u << sh) - 1) >> sh; (b << sh) < off + nch; ++b) {
+        if (b < I.icap) C.hitem[b] = (int32_t)slot;
+        else atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_CAPACITY);
+      }
+    } else {
+      atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_CAPACITY);
+    }
   }
 
   NPS_LAP(pc, 1);
@@ -788,6 +810,55 @@ __device__ __forceinline__ void walk_chunks(const InstDesc& I, const IterCtx& C,
     int4 cv, wv;
     load_chunk(I, act, c, ent.x, ent.y, cv, wv);
     relax_loaded(I, C, act, c, ent.x, ent.y, du, ent.z < 0, cv, wv, acc, S, lane);
+  }
+}
+
+// One work item of the grid-tier list L (cnt entries sorted by chunk offset):
+// chunks [kb, ke) of its flat chunk space, whose first chunk lies in entry js.
+// The warp loads 32 consecutive entries at a time (one coalesced load); each
+// lane finds the owner of its chunk among them with a 5-step shuffle search.
+// The owners' distances are read at walk time, one per window lane.
+// Every entry has at least one chunk, so a window of 32 entries covers any 32
+// consecutive chunks that start in its first entry.  Warp-collective.
+__device__ __forceinline__ void walk_item(const InstDesc& I, const IterCtx& C, const int4* L, uint32_t cnt,
+                                          uint32_t kb, uint32_t ke, uint32_t js, Acc& acc, Stage& S, int lane) {
+  uint32_t k = kb;
+  while (k < ke) {
+    const uint32_t jl = js + lane;
+    int4 E = make_int4(0, 0, 0, 0);
+    uint32_t off = 0xffffffffu, cov = 0xffffffffu, dv = kInf;
+    if (jl < cnt) {
+      E = L[jl];
+      off = (uint32_t)E.w;
+      cov = off + row_chunks(E.x, E.y);
+      const uint32_t v = (uint32_t)E.z & 0x7fffffffu;
+      if (v < (uint32_t)I.n) dv = __ldcg(I.dist + v);
+    }
+    const uint32_t lim = min(ke, __shfl_sync(kFull, cov, 31));  // end of the window's chunks
+    for (uint32_t k0 = k; k0 < lim; k0 += 32) {
+      const uint32_t kk = k0 + lane;
+      const bool act = kk < lim;
+      int o = 0;  // largest window index whose first chunk is <= kk (entry 0's is <= k0)
+#pragma unroll
+      for (int step = 16; step >= 1; step >>= 1) {
+        const uint32_t x = __shfl_sync(kFull, off, o + step);
+        if (x <= kk) o += step;
+      }
+      const int32_t s = __shfl_sync(kFull, E.x, o);
+      const int32_t e = __shfl_sync(kFull, E.y, o);
+      const int32_t z = __shfl_sync(kFull, E.z, o);
+      const uint32_t du = __shfl_sync(kFull, dv, o);
+      const uint32_t oo = __shfl_sync(kFull, off, o);
+      // the owner must hold chunk kk (it always does unless the list is inconsistent)
+      const bool own = kk >= oo && e > s && kk - oo < row_chunks(s, e);
+      if (act && !own) atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_CAPACITY);
+      const int32_t c = (s & ~3) + 4 * (int32_t)(kk - oo);
+      int4 cv, wv;
+      load_chunk(I, act && own, c, s, e, cv, wv);
+      relax_loaded(I, C, act && own, c, s, e, du, z < 0, cv, wv, acc, S, lane);
+    }
+    k = lim;
+    js += 32;
   }
 }
 
@@ -926,14 +997,17 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     C.heavy = I.heavy + ((it & 1) ? hhalf : 0);
     C.heavy_ctr = &ctr->heavy[it % 3];
     C.hcap = hhalf;
+    C.hitem = I.hitem + ((it & 1) ? I.icap : 0);
     C.split = (I.light_heavy && delta != 0) ? delta : 0u;
     C.heavy_iter = heavy_it;
     C.sq = (C.split != 0u && !heavy_it) ? I.sq[hg & 1] : nullptr;
     C.sq_tail = &ctr->stail[hg % 3];
     C.sstamp = base + hg + 1;
     C.local_rounds = heavy_it ? 0 : I.local_rounds;  // a heavy pass only relaxes heavy edges
+    C.order_deg = I.order_degree;
     level_thresholds(level, I.t1, I.t2, I.t3, C.t_warp, C.t_block, C.t_grid);
     const int4* Hprev = I.heavy + ((it & 1) ? 0 : hhalf);
+    const int32_t* Hitem = I.hitem + ((it & 1) ? 0 : I.icap);
 
     if (rank == 0 && threadIdx.x < kStripes) {
       ctr->work[(it + 1) % 3][threadIdx.x * 32] = 0;
@@ -957,7 +1031,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
 
     const int32_t* srcq = advance ? I.fq[ep & 1] : (heavy_it ? I.sq[hg & 1] : I.q[it & 1]);
     const uint32_t srclen = advance ? adv_len : (heavy_it ? slen : qlen);
-    const uint32_t n_heavy_items = (uint32_t)((hprev_tot + kHeavyItemChunks - 1) / kHeavyItemChunks);
+    const uint32_t n_heavy_items = (uint32_t)((hprev_tot + (1ull << I.item_shift) - 1) >> I.item_shift);
     const uint32_t n_items = n_heavy_items + (srclen + 31) / 32;
     Acc acc = {0, 0, 0, 0};
     Stage S;
@@ -1008,9 +1082,10 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
         }
         NPS_LAP(pc, 0);
         if (item < n_heavy_items) {
-          const unsigned long long kb = item * kHeavyItemChunks;
-          const unsigned long long ke = min(kb + kHeavyItemChunks, hprev_tot);
-          walk_chunks(I, C, Hprev, hprev_cnt, kb, ke, acc, S, lane);
+          const uint32_t kb = (uint32_t)item << I.item_shift;
+          const uint32_t ke = (uint32_t)min((unsigned long long)kb + (1ull << I.item_shift), hprev_tot);
+          const int32_t js = __ldcg(Hitem + item);
+          walk_item(I, C, Hprev, hprev_cnt, kb, ke, (uint32_t)js, acc, S, lane);
           NPS_LAP(pc, 4);
         } else {
           const uint32_t idx = (uint32_t)(item - n_heavy_items) * 32 + lane;

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -127,12 +128,41 @@ KernelFn pick_kernel(int bs, bool single) {
   }
 }
 
+// Shared-memory carveout: the smallest split that still holds `nb` resident
+// CTAs, so the rest of the SM's 256 KB of L1/shared storage caches the
+// distance array (the pre-check loads of hub vertices hit in L1 instead of
+// queueing on one L2 slice).  Done once per (device, kernel); occupancy is
+// checked again and the default restored if the split would lower it.
+cudaError_t set_carveout(int dev, KernelFn k, int bs, int nb) {
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> done;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!done.insert({dev, (const void*)k}).second) return cudaSuccess;
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, (const void*)k);
+  if (e != cudaSuccess) return e;
+  int smem_sm = 0, reserved = 0;
+  if ((e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev)) != cudaSuccess) return e;
+  if (smem_sm <= 0) return cudaSuccess;
+  const size_t need = (size_t)nb * (fa.sharedSizeBytes + (size_t)reserved);
+  int pct = (int)((need * 100 + (size_t)smem_sm - 1) / (size_t)smem_sm);
+  pct = std::min(100, std::max(1, pct));
+  if ((e = cudaFuncSetAttribute((const void*)k, cudaFuncAttributePreferredSharedMemoryCarveout, pct)) != cudaSuccess)
+    return e;
+  int nb2 = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, (const void*)k, bs, 0)) != cudaSuccess) return e;
+  if (nb2 < nb) return cudaFuncSetAttribute((const void*)k, cudaFuncAttributePreferredSharedMemoryCarveout, -1);
+  return cudaSuccess;
+}
+
 nps_status grid_size(int dev, const DevInfo& di, int bs, bool single, int ctas_per_sm, int* grid) {
   KernelFn k = pick_kernel(bs, single);
   if (!k) return nps_fail(NPS_ERR_INVALID_ARG, "block_size must be 128, 256 or 512");
   int nb = 0;
   NPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)k, bs, 0));
   if (nb <= 0) return nps_fail(NPS_ERR_CUDA, "persistent kernel does not fit on an SM");
+  NPS_CUDA(set_carveout(dev, k, bs, nb));
   if (ctas_per_sm > 0) nb = std::min(nb, ctas_per_sm);
   *grid = nb * di.sms;
   (void)dev;
@@ -312,6 +342,7 @@ nps_status check_params(const nps_params& p) {
   if (!(p.timeout_s > 0) || p.timeout_s > 3600) return nps_fail(NPS_ERR_INVALID_ARG, "timeout_s must be in (0, 3600]");
   if (p.delta >= NPS_INF) return nps_fail(NPS_ERR_INVALID_ARG, "delta must be < 2^30");
   if (p.local_rounds < 0 || p.local_rounds > 1024) return nps_fail(NPS_ERR_INVALID_ARG, "local_rounds must be in [0, 1024]");
+  if (p.order_degree < 0) return nps_fail(NPS_ERR_INVALID_ARG, "order_degree must be >= 0");
   return NPS_OK;
 }
 
@@ -344,6 +375,7 @@ void fill_thresholds(const nps_params& p, InstDesc& d) {
   d.policy = p.policy;
   d.light_heavy = p.light_heavy != 0;
   d.local_rounds = p.local_rounds;
+  d.order_degree = p.order_degree;
 }
 
 // Whole-launch bound: 30 per-wait timeouts, at least 60 s.
@@ -394,7 +426,9 @@ nps_status run_single(nps_ctx* c, cudaStream_t s, const int32_t* row, const int3
   if ((e = c->stamp.ensure(1, grow_marks || !c->stamp.p, s))) return e;
   if (grow_marks) NPS_CUDA(cudaMemsetAsync(c->stamp.p, 0, sizeof(uint32_t), s));
   const uint32_t hcap = heavy_capacity(n, m, p);
-  if ((e = c->heavy.ensure(hcap, false, s))) return e;
+  uint32_t icap = 0, ishift = 0;
+  nps_heavy_items(m, hcap / 2, 0, &icap, &ishift);
+  if ((e = c->heavy.ensure(nps_heavy_slots(hcap, icap), false, s))) return e;
   int grid = 0;
   if ((e = grid_size(c->device, c->di, p.block_size, true, p.ctas_per_sm, &grid))) return e;
   Control ctl(1, 1, grid);
@@ -426,6 +460,9 @@ nps_status run_single(nps_ctx* c, cudaStream_t s, const int32_t* row, const int3
   d.sq[0] = c->s0.p;
   d.sq[1] = c->s1.p;
   d.heavy = c->heavy.p;
+  d.hitem = (int32_t*)(c->heavy.p + hcap);
+  d.icap = icap;
+  d.item_shift = ishift;
   d.qcap = (uint32_t)n;
   d.hcap = hcap;
   d.ctr = ctl.ctr();
@@ -664,11 +701,12 @@ extern "C" nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, co
     c->b_graph = nullptr;
     // workspace: per instance 4 queues of n int32 + marks carved from pools
     size_t q_total = 0, h_total = 0;
-    std::vector<uint32_t> hcap(count);
+    std::vector<uint32_t> hcap(count), icap(count), ishift(count);
     for (int i = 0; i < count; ++i) {
       q_total += 6 * (size_t)inst[i].n;
       hcap[i] = heavy_capacity(inst[i].n, inst[i].m, p);
-      h_total += hcap[i];
+      nps_heavy_items(inst[i].m, hcap[i] / 2, 0, &icap[i], &ishift[i]);
+      h_total += nps_heavy_slots(hcap[i], icap[i]);
     }
     size_t mk_total = 0;
     for (int i = 0; i < count; ++i) mk_total += 3 * (size_t)inst[i].n;
@@ -753,8 +791,11 @@ extern "C" nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, co
       d.smark = c->b_stamp.p + mo;
       mo += x.n;
       d.heavy = c->b_heavy.p + ho;
+      d.hitem = (int32_t*)(c->b_heavy.p + ho + hcap[i]);
+      d.icap = icap[i];
+      d.item_shift = ishift[i];
       d.hcap = hcap[i];
-      ho += hcap[i];
+      ho += nps_heavy_slots(hcap[i], icap[i]);
       d.qcap = (uint32_t)x.n;
       d.ctr = ctl.ctr() + i;
       d.stamp_base = stamps + i;

@@ -14,6 +14,21 @@ void nps_clear_error();
 nps_status nps_build_csr(int32_t n, int64_t m, const int32_t* src, const int32_t* dst,
                          const uint32_t* w, bool dedupe, bool drop_self, nps_graph* out);
 
+// Work items of one half of the grid-tier list: its flat chunk space holds at
+// most m/4 + 2*entries chunks (row_chunks(s, e) <= (e - s)/4 + 2); an item is
+// 2^shift chunks, shift >= 6, the smallest that keeps the items within `cap`
+// (0 = no limit).
+inline void nps_heavy_items(int64_t m, uint64_t entries, uint64_t cap, uint32_t* icap, uint32_t* shift) {
+  const uint64_t chunks = (uint64_t)(m < 0 ? 0 : m) / 4 + 2 * entries + 1;
+  uint32_t sh = 6;
+  while (cap && (chunks >> sh) + 2 > cap) ++sh;
+  *shift = sh;
+  *icap = (uint32_t)((chunks >> sh) + 2);
+}
+
+// int4 slots of the grid-tier buffer: hcap entries, then 2 * icap item starts.
+inline size_t nps_heavy_slots(uint32_t hcap, uint32_t icap) { return (size_t)hcap + ((size_t)2 * icap + 3) / 4; }
+
 // Device copy of the learned-policy weights of `device` (null if none loaded).
 const void* nps_policy_device_weights(int device);
 

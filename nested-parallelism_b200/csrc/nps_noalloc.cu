@@ -57,7 +57,9 @@ constexpr size_t kOffStamp = align256(kOffTeam + sizeof(TeamDesc));
 constexpr size_t kOffMarks = align256(kOffStamp + sizeof(uint32_t));
 constexpr size_t kOffQueues = align256(kOffMarks + 3 * kMaxV * sizeof(uint32_t));
 constexpr size_t kOffHeavy = align256(kOffQueues + 6 * kMaxV * sizeof(int32_t));
-constexpr size_t kScratchBytes = align256(kOffHeavy + 2 * kMaxV * sizeof(int4));
+constexpr size_t kItemCap = 65536;  // grid-tier work items per half (larger items for larger m)
+constexpr size_t kOffItems = align256(kOffHeavy + 2 * kMaxV * sizeof(int4));
+constexpr size_t kScratchBytes = align256(kOffItems + 2 * kItemCap * sizeof(int32_t));
 static_assert(kScratchBytes <= NPS_NOALLOC_SCRATCH_BYTES, "scratch layout exceeds NPS_NOALLOC_SCRATCH_BYTES");
 
 }  // namespace
@@ -188,6 +190,8 @@ extern "C" nps_status nps_sssp_noalloc(const int32_t* d_row_ptr, const int32_t* 
   d.heavy = (int4*)(base + kOffHeavy);
   d.qcap = (uint32_t)nn;
   d.hcap = (uint32_t)(2 * nn);  // two halves of up to n grid-tier rows each
+  nps_heavy_items(m, nn, kItemCap, &d.icap, &d.item_shift);
+  d.hitem = (int32_t*)(base + kOffItems);
   d.ctr = ctr;
   d.stamp_base = (uint32_t*)(base + kOffStamp);
   d.trace = nullptr;  // no trace buffer: that would need an allocation
@@ -200,6 +204,7 @@ extern "C" nps_status nps_sssp_noalloc(const int32_t* d_row_ptr, const int32_t* 
   d.policy = p.policy;
   d.light_heavy = p.light_heavy != 0;
   d.local_rounds = p.local_rounds < 0 ? 0 : (p.local_rounds > 1024 ? 1024 : p.local_rounds);
+  d.order_degree = p.order_degree < 0 ? 0 : p.order_degree;
 
   const TeamDesc td{0, grid, 0, 1};
   LaunchParams lp;

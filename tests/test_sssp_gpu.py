@@ -257,7 +257,7 @@ def test_malformed_csr_is_reported_not_faulted(nps, oracle, cuda_device):
 
 
 def test_invalid_arguments(nps, cuda_device, uniform):
-    for kw in ({"level": 7}, {"block_size": 96}, {"threshold": 0}, {"timeout_s": 0.0}):
+    for kw in ({"level": 7}, {"block_size": 96}, {"threshold": 0}, {"timeout_s": 0.0}, {"order_degree": -1}):
         with pytest.raises(nps.NpsError) as ei:
             nps.sssp(uniform, 0, nps.Params(**kw))
         assert ei.value.status == 1
@@ -273,3 +273,21 @@ def test_warp_local_rounds(nps, oracle, cuda_device, rmat16, grid128, rounds, le
     for g in (rmat16, grid128):
         _check(nps, oracle, g, g.source, _p(nps, level=level, delta=delta, light_heavy=lh, local_rounds=rounds,
                                            threshold=32, block_threshold=128, grid_threshold=1024))
+
+
+@pytest.mark.parametrize("order_degree", [1, 4, 32, 100000])
+@pytest.mark.parametrize("level,delta,lh", [(2, 16, False), (2, 64, True), (3, 5, True), (1, 300, False)])
+def test_order_degree(nps, oracle, cuda_device, rmat16, grid128, order_degree, level, delta, lh):
+    """Improved vertices below order_degree join the current bucket whatever their
+    distance (only larger rows wait for their bucket); distances must not change."""
+    for g in (rmat16, grid128):
+        _check(nps, oracle, g, g.source, _p(nps, level=level, delta=delta, light_heavy=lh, order_degree=order_degree,
+                                           threshold=32, block_threshold=128, grid_threshold=1024))
+
+
+def test_grid_tier_small_threshold_items(nps, oracle, cuda_device, rmat16, uniform):
+    """Grid tier with threshold 1: rows of one chunk, so a work item spans many
+    list entries (several 32-entry windows per item)."""
+    for g in (rmat16, uniform):
+        for delta in (0, 50):
+            _check(nps, oracle, g, g.source, _p(nps, level=2, threshold=1, delta=delta))
