@@ -1,27 +1,36 @@
 #!/usr/bin/env python3
-"""SSSP throughput benchmark (GTEPS) of the B200 persistent consolidation kernel.
+"""SSSP throughput benchmark (GTEPS) of the B200 persistent consolidation kernel:
+the learned-policy kernel against the plain autotuned kernel on the same graph.
 
 Workload (default): R-MAT scale 22 (4,194,304 vertices), edge factor 16
 (67,108,864 generated edges, duplicates and self-loops removed), a=0.57 b=0.19
 c=0.19, uint32 weights uniform in [1,255], seeded synthetic graph (seed 1000),
 source = highest-out-degree vertex.  One step = one full SSSP from that source.
 
-  value    GTEPS = m_r / kernel time (m_r = out-edges of reached vertices), graph
+  plain    the autotuner picks fixed parameters on this graph (outside the timed
+           region); K steps of that configuration are timed first
+  value    GTEPS = m_r / kernel time (m_r = out-edges of reached vertices) of the
+           learned-policy kernel (nested-parallelism_b200/policy_weights.npz; the
+           plain parameters with the MLP choosing bucket widths and levels); graph
            resident in HBM, L2 flushed between steps, CUDA events on the launch stream
   e2e      the same metric through the public host-buffer call nps.sssp(): pinned
            host CSR -> device, kernel, distances -> host, every step
   roofline B_alg = 12 m_r + 12 n_r + 4 n bytes per SSSP over the measured HBM peak
   cpu_baseline  the reference's SSSP_CPU (heap Dijkstra, built from its sources
-           into oracle/_ref) timed on this host, one full SSSP of the workload
+           into oracle/_ref) timed on this host, one full SSSP of the workload;
+           its distances must equal both GPU arms'
 
 `--impl reference` times the reference's CPU SSSP (oracle/_ref, else the oracle
 restatement) on all host cores: the K steps run concurrently, one process each.
-Multi-GPU (torchrun): replicas only -- every rank solves its own copy, the
-value is the sum of edges over the max device time across ranks.
+Multi-GPU (torchrun): replicas only for one graph -- every rank solves its own
+copy, the value is the sum of edges over the max device time across ranks;
+`--workload batch64` shards the 64-instance batch over the ranks instead.
 """
 from __future__ import annotations
 
 import argparse
+import contextlib
+import dataclasses
 import importlib
 import json
 import os
@@ -46,9 +55,14 @@ WORKLOADS = {
                  "4096x4096 4-neighbour grid, 5% pairs dropped, w in [1,1000], seed 1, source (0,0)"),
     "uniform16k": ("uniform", dict(n=16384, m=131072, wmax=100, seed=1),
                    "uniform random 16,384 vertices / 131,072 edges, w in [1,100], seed 1, source 0"),
+    "batch64": ("batch", dict(count=64, seed=7),
+                "64 R-MAT instances (a=.57 b=.19 c=.19), scale U{12..18}, edge factor {4,8,16,32}, "
+                "w in [1,255], random sources, seed 7; one persistent CUDA-graph launch per shard"),
 }
 
-# plain autotuned parameters per workload class (overridden by --delta/--level)
+METRIC = "SSSP GTEPS on 1 B200: learned-policy vs plain, % of HBM roofline, bit-exact"
+
+# autotuner seed configuration per workload class (--delta / --level pin it instead)
 DEFAULT_PARAMS = {
     "rmat": dict(level=2, threshold=64, delta=0, block_size=512),
     "grid": dict(level=2, threshold=64, delta=4096, block_size=256),
@@ -202,6 +216,202 @@ def run_reference(a, nps, g, m_r, n_r, cfg):
 
 
 # ---------------------------------------------------------------------------
+# batched workload: every rank solves its LPT shard of the 64 instances in one
+# persistent launch replayed from a CUDA graph (weak in instances per launch,
+# no exchange during the solve; results all-gathered at the end)
+
+BATCH_AXES = {"level": [1, 2, 3], "threshold": [32, 64, 128], "delta": [0, 32, 128, 1024],
+              "block_size": [256, 512]}
+
+
+def _batch_reference(a, B, count, seed, cfg):
+    """--impl reference for the batch: the reference's SSSP_CPU over all instances,
+    one process per host core, each step = the whole batch."""
+    import multiprocessing as mp
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    use_ref = oracle.have_reference()
+    items = B.rmat_batch(count, seed)
+    m_r_total = 0
+    with tempfile.TemporaryDirectory(dir="/dev/shm" if os.path.isdir("/dev/shm") else None) as td:
+        paths = []
+        for it in items:
+            d0 = oracle.sssp_heap(it.graph.row_ptr, it.graph.col, it.graph.w, it.source)
+            m_r_total += oracle.reached(it.graph.row_ptr, d0)[1]
+            path = os.path.join(td, f"g{it.index}.npz")
+            np.savez(path, row=it.graph.row_ptr, col=it.graph.col, w=it.graph.w, src=it.source)
+            paths.append(path)
+        cores = os.cpu_count() or 1
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(min(cores, count)) as pool:
+            for _ in range(a.warmup):
+                pool.map(_batch_ref_worker, [(p, use_ref) for p in paths[:min(cores, count)]], chunksize=1)
+            t0 = time.perf_counter()
+            for _ in range(a.steps):
+                pool.map(_batch_ref_worker, [(p, use_ref) for p in paths], chunksize=1)
+            wall = time.perf_counter() - t0
+    value = a.steps * m_r_total / wall / 1e9
+    return {"impl": "reference", "metric": "sssp_batch_gteps", "value": value, "unit": "GTEPS", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * wall / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": min(cores, count),
+                             "kind": "reference" if use_ref else "port",
+                             "sample": f"each step: all {count} instances, one SSSP_CPU per instance, "
+                                       f"{min(cores, count)} processes"},
+            "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def _batch_ref_worker(args):
+    path, use_ref = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    z = np.load(path)
+    if use_ref:
+        d, t = oracle.ref_sssp_cpu(z["row"], z["col"], z["w"], int(z["src"]))
+    else:
+        d, t = oracle.timed(oracle.sssp_heap, z["row"], z["col"], z["w"], int(z["src"]))
+    return t
+
+
+def bench_batch(a, nps, ws, rank, local, desc):
+    import torch
+    import torch.distributed as dist
+    B = importlib.import_module("nested-parallelism_b200.batch")
+    at = importlib.import_module("nested-parallelism_b200.autotune")
+    _, args, _ = WORKLOADS[a.workload]
+    count, seed = args["count"], args["seed"]
+    cfg = {"workload": a.workload, "description": desc, "instances": count}
+    if a.impl == "reference":
+        if rank == 0:
+            cfg["parallelism"] = "host cores"
+            print(json.dumps(_batch_reference(a, B, count, seed, cfg)))
+        return 0
+    if ws > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    mine = B.shard_indices(count, seed, ws, rank)
+    items = B.rmat_batch(count, seed, only=mine)
+    dgs = [at.to_device(it.graph, it.source, dev) for it in items]
+    params, tune_ms, tune_log = at.autotune(dgs, repeats=2, budget=a.tune_budget, axes=BATCH_AXES, batch=True)
+    params.device = local
+    insts = [nps.Instance(d.row_ptr, d.col, d.w, d.dist, d.n, d.m, d.src) for d in dgs]
+    stream = torch.cuda.Stream(dev)
+    sptr = stream.cuda_stream
+    with torch.cuda.stream(stream):
+        for _ in range(a.warmup):
+            nps.sssp_batch(insts, params, use_graph=True, stream=sptr)
+    torch.cuda.synchronize(dev)
+    dists = [d.dist.cpu().numpy().view(np.uint32).copy() for d in dgs]
+    m_r = n_r = 0
+    b_alg = 0
+    for it, dd in zip(items, dists):
+        reached = dd < nps.INF
+        mr = int(np.diff(it.graph.row_ptr)[reached].sum())
+        nr = int(reached.sum())
+        m_r += mr
+        n_r += nr
+        b_alg += 12 * mr + 12 * nr + 4 * it.graph.n
+    flush = torch.empty(256 << 20, dtype=torch.int8, device=dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            for i in range(a.steps):
+                flush.fill_(i & 0x7F)
+                evs[i][0].record(stream)
+                nps.sssp_batch(insts, params, use_graph=True, stream=sptr)
+                evs[i][1].record(stream)
+        torch.cuda.synchronize(dev)
+    if ws > 1:
+        dist.barrier()
+    kern_ms = sum(s.elapsed_time(e) for s, e in evs)
+    clocks = clk.summary()
+
+    # e2e: host CSR (pinned) -> device, one batch launch, distances -> host, every step
+    host = []
+    for it in items:
+        g = it.graph
+        host.append([torch.from_numpy(np.ascontiguousarray(x).view(np.int32)).pin_memory()
+                     for x in (g.row_ptr, g.col, g.w)] + [torch.empty(g.n, dtype=torch.int32).pin_memory()])
+    h2d = sum(sum(t.numel() * 4 for t in h[:3]) for h in host)
+    d2h = sum(h[3].numel() * 4 for h in host)
+    e2e_steps = a.e2e_steps or a.steps
+
+    def e2e_step():
+        with torch.cuda.stream(stream):
+            for h, d in zip(host, dgs):
+                d.row_ptr.copy_(h[0], non_blocking=True)
+                d.col.copy_(h[1], non_blocking=True)
+                d.w.copy_(h[2], non_blocking=True)
+            nps.sssp_batch(insts, params, use_graph=True, stream=sptr)
+            for h, d in zip(host, dgs):
+                h[3].copy_(d.dist, non_blocking=True)
+        stream.synchronize()
+
+    e2e_step()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    e2e_ok = all(np.array_equal(h[3].numpy().view(np.uint32), dd) for h, dd in zip(host, dists))
+
+    tot = torch.tensor([kern_ms, e2e_ms, float(m_r), float(b_alg)], dtype=torch.float64, device=dev)
+    mx = tot.clone()
+    sm = tot.clone()
+    if ws > 1:
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    kern_max, e2e_max, m_r_all = float(mx[0]), float(mx[1]), float(sm[2])
+    results = B.gather_results([{"index": it.index, "fnv1a": nps.fnv1a(dd)} for it, dd in zip(items, dists)])
+
+    cpu = None
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        t_cpu = 0.0
+        m_s = 0
+        exact = True
+        sample = items[:8]
+        for it, dd in zip(sample, dists[:8]):
+            if oracle.have_reference():
+                ref, t = oracle.ref_sssp_cpu(it.graph.row_ptr, it.graph.col, it.graph.w, it.source)
+            else:
+                ref, t = oracle.timed(oracle.sssp_heap, it.graph.row_ptr, it.graph.col, it.graph.w, it.source)
+            t_cpu += t
+            m_s += int(np.diff(it.graph.row_ptr)[ref < nps.INF].sum())
+            exact = exact and bool(np.array_equal(ref, dd))
+        cpu = {"value": m_s / t_cpu / 1e9, "unit": "GTEPS", "cores": 1,
+               "kind": "reference" if oracle.have_reference() else "port",
+               "sample": "instances 0..7 of the batch, one SSSP_CPU each, 1 thread", "seconds": t_cpu,
+               "bit_exact_vs_gpu": exact}
+    peak, peak_src = load_peaks()
+    per_launch = kern_ms / a.steps * 1e-3
+    if rank == 0:
+        cfg.update({"parallelism": f"{ws} shards (LPT by n + edges)" if ws > 1 else "1 GPU",
+                    "instances_rank0": len(items), "m_reached": int(m_r_all), "params": dataclasses.asdict(params),
+                    "autotune": {"evaluations": len(tune_log), "best_ms": tune_ms},
+                    "l2": "flushed between steps (256 MB write)", "result_hashes": len(results)})
+        line = {"metric": "sssp_batch_gteps", "value": a.steps * m_r_all / (kern_max * 1e-3) / 1e9, "unit": "GTEPS",
+                "n_gpus": ws, "steps": a.steps, "warmup": a.warmup, "ms_per_step": kern_max / a.steps,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32",
+                "data": "synthetic", "config": cfg,
+                "roofline": {"bound": "hbm", "achieved": b_alg / per_launch / 1e9, "peak": peak, "unit": "GB/s",
+                             "frac": b_alg / per_launch / 1e9 / peak, "traffic": None, "peak_source": peak_src,
+                             "b_alg_bytes": b_alg},
+                "e2e": {"value": m_r_all / (e2e_max * 1e-3) / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h, "ms_per_step": e2e_max, "bit_exact_vs_device_run": e2e_ok,
+                        "call": "sssp_batch on device copies of pinned host CSR, distances back to pinned host"},
+                "gpu_launches": a.steps, "clocks": clocks, "cpu_baseline": cpu}
+        print(json.dumps(line))
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
 
 def main():
     ap = argparse.ArgumentParser()
@@ -212,15 +422,18 @@ def main():
     ap.add_argument("--workload", default="rmat22", choices=sorted(WORKLOADS))
     ap.add_argument("--delta", type=int, default=None)
     ap.add_argument("--level", type=int, default=None)
-    ap.add_argument("--policy", default="plain", choices=["plain", "learned"])
+    ap.add_argument("--policy", default="learned", choices=["plain", "learned"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--tune-budget", type=int, default=24, help="autotuner evaluations before timing")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
 
     ws, rank, local = dist_env()
     nps = importlib.import_module("nested-parallelism_b200")
     kind, _, desc = WORKLOADS[a.workload]
+    if kind == "batch":
+        return bench_batch(a, nps, ws, rank, local, desc)
     prm = dict(DEFAULT_PARAMS[kind])
     if a.delta is not None:
         prm["delta"] = a.delta
@@ -247,58 +460,79 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    at = importlib.import_module("nested-parallelism_b200.autotune")
+    pol = importlib.import_module("nested-parallelism_b200.policy")
 
     g = make_graph(nps, a.workload)
-    params = nps.Params(device=local, **prm)
-    if a.policy == "learned":
-        from importlib import import_module
-        pol = import_module("nested-parallelism_b200.policy")
-        wpath = os.path.join(ROOT, "nested-parallelism_b200", "policy_weights.npz")
+    dg = at.to_device(g, device=dev)
+    row, col, w, dist_t = dg.row_ptr, dg.col, dg.w, dg.dist
+
+    # plain autotuned configuration: the autotuner on this graph (outside the timed region),
+    # unless --delta / --level pin it
+    tune_log = []
+    if a.tune_budget > 0 and a.delta is None and a.level is None:
+        seed_p = nps.Params(device=local, **prm)
+        plain, _, tune_log = at.autotune([dg], repeats=3, budget=a.tune_budget, seed=seed_p)
+        plain.device = local
+    else:
+        plain = nps.Params(device=local, **prm)
+    wpath = os.path.join(ROOT, "nested-parallelism_b200", "policy_weights.npz")
+    use_learned = a.policy == "learned" and os.path.exists(wpath)
+    learned = None
+    if use_learned:
         pol.load_into_kernel(pol.MLPWeights.load(wpath), local)
-        params.policy = nps.POLICY_LEARNED
+        learned = dataclasses.replace(plain, policy=nps.POLICY_LEARNED, light_heavy=False, order_degree=0,
+                                      delta_schedule=0)
+    params = learned if use_learned else plain
 
-    def to_dev(x):
-        return torch.from_numpy(np.ascontiguousarray(x).view(np.int32)).to(dev)
-
-    row, col, w = to_dev(g.row_ptr), to_dev(g.col), to_dev(g.w)
-    dist_t = torch.empty(g.n, dtype=torch.int32, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.int8, device=dev)  # > 126 MB L2
     stream = torch.cuda.Stream(dev)
     sptr = stream.cuda_stream
 
-    def step():
-        return nps.sssp_device(row, col, w, g.n, g.m, g.source, dist_t, params, stream=sptr)
+    def step(p):
+        return nps.sssp_device(row, col, w, g.n, g.m, g.source, dist_t, p, stream=sptr)
 
-    with torch.cuda.stream(stream):
-        for _ in range(a.warmup):
-            st = step()
-    torch.cuda.synchronize(dev)
-    dh = dist_t.cpu().numpy().view(np.uint32)
-    reached = dh < nps.INF
+    def timed(p, clk=None):
+        """W warm-up steps, then K steps with an L2 flush before each; CUDA events
+        on the launch stream around each SSSP.  Returns (per-step ms, stats, dist)."""
+        with torch.cuda.stream(stream):
+            for _ in range(a.warmup):
+                step(p)
+        torch.cuda.synchronize(dev)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(a.steps)]
+        stats = []
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        ctx = clk if clk is not None else contextlib.nullcontext()
+        with ctx:
+            with torch.cuda.stream(stream):
+                for i in range(a.steps):
+                    flush.fill_(i & 0x7F)
+                    evs[i][0].record(stream)
+                    stats.append(step(p))
+                    evs[i][1].record(stream)
+            torch.cuda.synchronize(dev)
+        if ws > 1:
+            dist.barrier()
+        return [s.elapsed_time(e) for s, e in evs], stats, dist_t.cpu().numpy().view(np.uint32).copy()
+
+    # plain arm first (its distances define reached vertices), then the headline arm
+    plain_ms, plain_stats, d_plain = timed(plain)
+    reached = d_plain < nps.INF
     n_r = int(reached.sum())
     m_r = int(np.diff(g.row_ptr)[reached].sum())
     b_alg = 12 * m_r + 12 * n_r + 4 * g.n
-
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
-    stats = []
-    if ws > 1:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
-    with ClockSampler(local) as clk:
-        wall0 = time.perf_counter()
-        with torch.cuda.stream(stream):
-            for i in range(a.steps):
-                flush.fill_(i & 0x7F)
-                evs[i][0].record(stream)
-                stats.append(step())
-                evs[i][1].record(stream)
-        torch.cuda.synchronize(dev)
-        wall = time.perf_counter() - wall0
-    if ws > 1:
-        dist.barrier()
-    step_ms = [s.elapsed_time(e) for s, e in evs]
-    kern_ms = sum(step_ms)
+    if use_learned:
+        clk = ClockSampler(local)
+        step_ms, stats, dh = timed(learned, clk)
+    else:
+        clk = ClockSampler(local)
+        step_ms, stats, dh = timed(plain, clk)
     clocks = clk.summary()
+    kern_ms = sum(step_ms)
+    exact_vs_plain = bool(np.array_equal(dh, d_plain))
 
     # ---- e2e through the host-buffer public call (pinned host memory)
     def pinned(x):
@@ -318,11 +552,12 @@ def main():
     e2e_wall = (time.perf_counter() - t0) / e2e_steps
     e2e_ok = bool((hout == dh).all())
 
-    tot_t = torch.tensor([kern_ms, e2e_wall * 1e3], dtype=torch.float64, device=dev)
+    tot_t = torch.tensor([kern_ms, e2e_wall * 1e3, sum(plain_ms)], dtype=torch.float64, device=dev)
     if ws > 1:
         dist.all_reduce(tot_t, op=dist.ReduceOp.MAX)
-    kern_ms_max, e2e_ms_max = float(tot_t[0]), float(tot_t[1])
+    kern_ms_max, e2e_ms_max, plain_ms_max = float(tot_t[0]), float(tot_t[1]), float(tot_t[2])
     value = ws * a.steps * m_r / (kern_ms_max * 1e-3) / 1e9
+    plain_value = ws * a.steps * m_r / (plain_ms_max * 1e-3) / 1e9
     e2e_value = ws * m_r / (e2e_ms_max * 1e-3) / 1e9
 
     peak, peak_src = load_peaks()
@@ -332,7 +567,8 @@ def main():
     tr_path = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tr_path):
         with open(tr_path) as f:
-            traffic = json.load(f).get(a.workload)
+            tr = json.load(f)
+        traffic = tr.get(a.workload + ("_learned" if use_learned else ""))
 
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
@@ -348,20 +584,31 @@ def main():
             kind_cpu = "port"
             sample = "one full SSSP of the workload by the oracle's restated heap Dijkstra, 1 thread"
         cpu = {"value": m_r / tcpu / 1e9, "unit": "GTEPS", "cores": 1, "kind": kind_cpu, "sample": sample,
-               "seconds": tcpu, "bit_exact_vs_gpu": bool((dref == dh).all())}
+               "seconds": tcpu, "bit_exact_vs_gpu": bool((dref == dh).all() and (dref == d_plain).all())}
 
     if rank == 0:
+        st = stats[-1]
         line = {
-            "metric": "sssp_gteps", "value": value, "unit": "GTEPS", "n_gpus": ws, "steps": a.steps,
+            "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": ws, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": kern_ms_max / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
             "config": {"workload": a.workload, "description": desc, "n": g.n, "m": g.m, "m_reached": m_r,
-                       "n_reached": n_r, "source": g.source, "params": prm, "policy": a.policy,
+                       "n_reached": n_r, "source": g.source,
+                       "policy": "learned" if use_learned else "plain",
+                       "params": dataclasses.asdict(params),
                        "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
                        "l2": "flushed between steps (256 MB write); CSR 12 B/edge also exceeds L2",
-                       "iterations": stats[-1].iterations, "buckets": stats[-1].buckets,
-                       "edges_scanned": stats[-1].edges_scanned, "grid_ctas": stats[-1].grid_ctas,
-                       "step_ms_min": min(step_ms), "step_ms_max": max(step_ms), "wall_s": wall},
+                       "iterations": st.iterations, "buckets": st.buckets,
+                       "edges_scanned": st.edges_scanned, "grid_ctas": st.grid_ctas,
+                       "step_ms_min": min(step_ms), "step_ms_max": max(step_ms),
+                       "autotune_evaluations": len(tune_log)},
+            "plain": {"value": plain_value, "unit": "GTEPS", "ms_per_step": plain_ms_max / a.steps,
+                      "params": dataclasses.asdict(plain), "iterations": plain_stats[-1].iterations,
+                      "edges_scanned": plain_stats[-1].edges_scanned,
+                      "note": "plain autotuned kernel (fixed parameters, no policy), same graph, same timing"},
+            "learned_over_plain": (value / plain_value) if use_learned else None,
+            "bit_exact": {"learned_vs_plain": exact_vs_plain,
+                          "vs_cpu_dijkstra": cpu["bit_exact_vs_gpu"] if cpu else None},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                          "b_alg_bytes": b_alg, "b_alg_formula": "12*m_r + 12*n_r + 4*n"},

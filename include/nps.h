@@ -93,7 +93,10 @@ typedef struct nps_params {
   int32_t order_degree;     /* with delta > 0: an improved vertex whose out-degree is below this
                                joins the current bucket whatever its distance, so only rows of at
                                least this degree wait for their bucket (0 = every vertex waits) */
-  int32_t reserved[4];      /* reserved[0] = 1: test hook, the first in-kernel barrier waits for an
+  uint32_t delta_schedule;  /* 0: every bucket is delta wide.  Otherwise bucket b (0 = the first)
+                               is 2^k wide with k = bits [4b, 4b+4) for b < 7 and bits [28, 32)
+                               for every later bucket; delta is then unused (plain policy only) */
+  int32_t reserved[3];      /* reserved[0] = 1: test hook, the first in-kernel barrier waits for an
                                arrival that never comes, so its bounded wait must expire */
 } nps_params;
 

@@ -37,7 +37,7 @@ __all__ = [
     "CONSOLIDATE_HYBRID", "POLICY_PLAIN", "POLICY_LEARNED", "Graph", "Params", "Stats",
     "NpsError", "gen_uniform", "gen_rmat", "gen_grid", "convertCSR", "readInputDIMACS9",
     "readInputDIMACS10", "readInputSLNDC", "writeDIMACS9", "sssp", "sssp_device", "SSSP_GPU",
-    "sssp_np_consolidate_gpu", "sssp_batch", "trace_read", "fnv1a", "abi_version", "lib",
+    "sssp_np_consolidate_gpu", "sssp_batch", "trace_read", "fnv1a", "delta_schedule", "abi_version", "lib",
 ]
 
 
@@ -171,6 +171,19 @@ def writeDIMACS9(path: str, g: Graph, source: Optional[int] = None) -> None:
           "writeDIMACS9")
 
 
+def delta_schedule(first, rest: int) -> int:
+    """Params.delta_schedule word: bucket b < len(first) is 2**first[b] wide (at most
+    7 entries), every later bucket 2**rest.  Exponents are 0..15."""
+    ks = list(first)
+    if len(ks) > 7 or not all(0 <= k <= 15 for k in ks + [rest]):
+        raise ValueError("at most 7 leading exponents, each in 0..15")
+    ks = ks + [rest] * (7 - len(ks))
+    word = 0
+    for b, k in enumerate(ks + [rest]):
+        word |= int(k) << (4 * b)
+    return word
+
+
 def fnv1a(dist: np.ndarray) -> int:
     a = np.ascontiguousarray(dist, dtype=np.uint32)
     return int(lib.nps_fnv1a_u32(a.ctypes.data, a.shape[0]))
@@ -195,6 +208,7 @@ class Params:
     light_heavy: bool = True            # delta > 0: heavy edges (w >= delta) relaxed once per bucket
     local_rounds: int = 0               # warp-local rounds on just-improved vertices per work item
     order_degree: int = 0               # delta > 0: rows below this degree ignore the bucket bound
+    delta_schedule: int = 0             # per-bucket log2 widths, 4 bits each (see delta_schedule())
     fault_inject_wait: bool = False     # test hook: the first barrier can never complete
 
     def to_c(self, device_ptrs: bool, stream: Optional[int] = None) -> nps_params:
@@ -208,6 +222,7 @@ class Params:
         p.light_heavy = int(bool(self.light_heavy))
         p.local_rounds = int(self.local_rounds)
         p.order_degree = int(self.order_degree)
+        p.delta_schedule = int(self.delta_schedule) & 0xFFFFFFFF
         p.device_ptrs = int(bool(device_ptrs))
         p.stream = stream
         p.reserved[0] = int(bool(self.fault_inject_wait))

@@ -1,8 +1,8 @@
 """Autotuner for the persistent SSSP kernel's parameters.
 
 Picks the consolidation level and degree thresholds, the block shape (threads
-per CTA, CTAs per SM), the bucket width delta, the light/heavy split and the
-warp-local rounds for a class of graphs by timing the CUDA kernel itself on
+per CTA, CTAs per SM), the bucket width delta, the light/heavy split, the
+degree ordering of bucket bounds and the warp-local rounds for a class of graphs by timing the CUDA kernel itself on
 sample graphs (device-resident, CUDA-event kernel times, median of repeats).
 
 Search: coordinate descent over a discrete space.  Starting from a seed
@@ -37,9 +37,10 @@ AXES: Dict[str, List] = {
     "delta": [0, 8, 16, 32, 64, 128, 256, 1024, 4096, 16384, 65536],
     "light_heavy": [False, True],
     "local_rounds": [0, 2, 8],
+    "order_degree": [0, 32, 128],
 }
-ORDER = ["delta", "level", "threshold", "light_heavy", "grid_threshold", "block_size", "local_rounds",
-         "ctas_per_sm"]
+ORDER = ["delta", "level", "threshold", "light_heavy", "order_degree", "grid_threshold", "block_size",
+         "local_rounds", "ctas_per_sm"]
 
 
 @dataclasses.dataclass
@@ -145,8 +146,8 @@ class Autotuner:
                         continue
                     if name == "grid_threshold" and best.level != 3:
                         continue  # only the hybrid level uses it
-                    if name == "light_heavy" and best.delta == 0:
-                        continue
+                    if name in ("light_heavy", "order_degree") and best.delta == 0:
+                        continue  # both act on bucket bounds only
                     cand = _normalise(dataclasses.replace(best, **{name: val}))
                     ms = self.evaluate(cand)
                     if ms < best_ms * 0.995:

@@ -121,6 +121,7 @@ struct InstDesc {
   int32_t light_heavy;  // 1: split edges at delta (relax w >= delta once per settled vertex)
   int32_t local_rounds; // warp-local processing rounds per vertex item (0 = none)
   int32_t order_degree; // rows below this degree ignore the bucket bound (0 = none)
+  uint32_t dsched;      // per-bucket log2 widths, 4 bits each (0 = fixed delta)
 };
 
 struct TeamDesc {
@@ -871,7 +872,7 @@ __device__ __forceinline__ float bf16_bits_to_float(uint16_t b) {
 }
 
 template <int BS>
-__device__ __forceinline__ void policy_eval(const PolicyDev* pol, Smem<BS>& sm) {
+__device__ __noinline__ void policy_eval(const PolicyDev* pol, Smem<BS>& sm) {
   const int t = threadIdx.x;
   __syncthreads();
   if (t < NPS_MLP_HID) {
@@ -964,7 +965,23 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
   __syncthreads();
   uint32_t qlen = min(sm.bc_q, I.qcap);
   uint32_t it = 0, ep = 0;
-  uint32_t delta = I.delta;
+  uint32_t delta = I.dsched ? 1u << (I.dsched & 15u) : I.delta;
+  int level = I.level;
+  if (learned) {
+    // the first bucket's width and the first level come from the policy too, on the
+    // start state: log2(1 + frontier), no degree histogram, no advances, 1 of n reached
+    if (threadIdx.x == 0) {
+      for (int i = 0; i < NPS_MLP_IN; ++i) {
+        float f = 0.f;
+        if (i == 0) f = log2f(1.f + (float)qlen);
+        if (i == 10) f = 1.f / (float)I.n;
+        sm.feat[i] = (f - P.policy->mean[i]) * P.policy->istd[i];
+      }
+    }
+    policy_eval<BS>(P.policy, sm);
+    delta = 1u << sm.pol_choice[0];
+    level = sm.pol_choice[1];
+  }
   uint32_t T = delta == 0 ? 0xffffffffu : delta;
   bool advance = false;
   bool heavy_it = false;  // this iteration relaxes the heavy edges of the settle list
@@ -973,7 +990,6 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
   uint32_t adv_len = 0, T_old = 0;
   uint32_t hprev_cnt = 0;
   unsigned long long hprev_tot = 0;
-  int level = I.level;
   Acc tot = {0, 0, 0, 0};
   PhaseClock pc;
   pc.reset();
@@ -1236,7 +1252,12 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
         break;
       }
       // bucket advance: the next iteration filters the far pile of epoch ep
-      if (learned) delta = 1u << sm.pol_choice[0];
+      if (learned) {
+        delta = 1u << sm.pol_choice[0];
+      } else if (I.dsched) {
+        const uint32_t b = min(buckets + 1u, 7u);  // index of the bucket this advance opens
+        delta = 1u << ((I.dsched >> (4u * b)) & 15u);
+      }
       const uint32_t fm = sm.bc_m;
       const uint32_t dstep = delta ? delta : 1u;
       unsigned long long nt = (unsigned long long)T + dstep;

@@ -376,6 +376,7 @@ void fill_thresholds(const nps_params& p, InstDesc& d) {
   d.light_heavy = p.light_heavy != 0;
   d.local_rounds = p.local_rounds;
   d.order_degree = p.order_degree;
+  d.dsched = p.delta_schedule;
 }
 
 // Whole-launch bound: 30 per-wait timeouts, at least 60 s.

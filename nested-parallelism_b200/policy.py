@@ -1,9 +1,9 @@
 """Learned per-iteration policy for the persistent SSSP kernel.
 
 A 2-layer MLP (12 features -> 32 ReLU -> 14 logits; bf16 weights, fp32
-accumulation) picks, at every bucket advance, the next bucket width
-delta = 2^k (k = 0..10) and, at every iteration, the consolidation level
-(warp / block / grid).  Inference runs inside the persistent kernel
+accumulation) picks the width delta = 2^k (k = 0..10) of the first bucket
+(from the start state) and of every bucket a bucket advance opens, and, at
+every iteration, the consolidation level (warp / block / grid).  Inference runs inside the persistent kernel
 (policy_eval in csrc/nps_device.cuh); training runs on the GPU through the
 forward / loss-backward / Adam kernels of csrc/nps_mlp.cu.  Device memory is
 plain torch tensors; all arithmetic is in those kernels.
@@ -160,84 +160,97 @@ def smoke_step(device) -> float:
 
 
 # ---------------------------------------------------------------------------
-# Training data from traces of plain runs.
+# Training data: imitation of the best bucket schedule of the plain kernel.
 #
-# For every training graph the plain kernel runs once per fixed configuration
-# (delta in DELTA_CHOICES x level in LEVEL_CHOICES, the other parameters those
-# of the plain autotuned configuration) with tracing on.  A trace record holds
-# the kernel's own feature vector after an iteration and the device time at
-# which the iteration ended.  Each record is placed in a progress bin (reached
-# vertices at that point over the reached total); the cost of a configuration
-# in a bin is the device time of the iterations that start in it.  Every record
-# of a graph is labelled with the configuration that is cheapest in the
-# record's bin, weighted by how much that choice saves there against the median
-# configuration.  The network so learns which bucket width and consolidation
-# level pay off in which phase of a run.
+# The plain kernel runs a fixed bucket width, or a scripted per-bucket width
+# schedule (Params.delta_schedule).  For every training graph a teacher search
+# times the plain kernel under each candidate schedule (a few narrow leading
+# buckets, then wide ones) and under each consolidation level, keeps the
+# fastest, and runs it once more with tracing on.  Every trace record holds the
+# kernel's own feature vector after an iteration; the record that precedes a
+# bucket advance is labelled with the log2 width the schedule gave the bucket
+# that advance opened, and every record with the best level.  The start state
+# (before the first iteration) is labelled with the first bucket's width.  The
+# network so learns, from frontier statistics alone, when narrow buckets pay
+# for their extra iterations and when the run should go unordered.
 
-DELTA_CHOICES = [1 << k for k in range(11)]
 LEVEL_CHOICES = [0, 1, 2]
-PROGRESS_BINS = np.array([0.0, 1e-3, 1e-2, 0.05, 0.2, 0.5, 0.8, 0.95, 0.99, 1.01])
+LEADING_K = (0, 1, 2, 3)   # log2 widths tried for the leading buckets
+REST_K = (8, 10)           # log2 width of every later bucket
 
 
-def trace_run(dg, params, device: int = 0):
-    """One traced run on a device-resident graph; returns (kernel_ms, records)."""
+def candidate_schedules(max_lead: int = 4):
+    """(leading exponents, rest exponent) pairs: non-decreasing leading widths,
+    1..max_lead of them, then a wide remainder."""
+    import itertools
+    out = []
+    for n in range(1, max_lead + 1):
+        for lead in itertools.combinations_with_replacement(LEADING_K, n):
+            for r in REST_K:
+                out.append((tuple(lead), r))
+    return out
+
+
+def schedule_params(base, lead, rest, level=None):
+    import dataclasses as _dc
+    from . import delta_schedule
+    kw = dict(delta_schedule=delta_schedule(list(lead), rest), policy=0, light_heavy=False, order_degree=0)
+    if level is not None:
+        kw["level"] = level
+    return _dc.replace(base, **kw)
+
+
+def _time(dg, params, reps: int = 3) -> float:
+    from . import sssp_device
+    sssp_device(dg.row_ptr, dg.col, dg.w, dg.n, dg.m, dg.src, dg.dist, params)  # warm-up
+    ts = [sssp_device(dg.row_ptr, dg.col, dg.w, dg.n, dg.m, dg.src, dg.dist, params).kernel_ms
+          for _ in range(reps)]
+    return float(np.median(ts))
+
+
+def teacher_search(dg, base, schedules, reps: int = 3):
+    """Fastest (schedule, level) for one device graph.  Returns
+    (best_ms, (lead, rest), level, {schedule: ms})."""
+    times = {}
+    for lead, rest in schedules:
+        times[(lead, rest)] = _time(dg, schedule_params(base, lead, rest), reps)
+    best = min(times, key=times.get)
+    lv_ms = {lv: _time(dg, schedule_params(base, best[0], best[1], lv), reps) for lv in LEVEL_CHOICES}
+    level = min(lv_ms, key=lv_ms.get)
+    return lv_ms[level], best, level, times
+
+
+def start_features(n: int, frontier: int = 1) -> np.ndarray:
+    """The start-state features the kernel evaluates before its first iteration."""
+    f = np.zeros(IN, np.float32)
+    f[0] = np.log2(1.0 + frontier)
+    f[10] = 1.0 / n
+    return f
+
+
+def trace_schedule(dg, base, lead, rest, level, device: int = 0):
+    """One traced plain run under a schedule; returns its trace records."""
     import dataclasses as _dc
     from . import sssp_device, trace_read
-    p = _dc.replace(params, trace=True, policy=0)
-    st = sssp_device(dg.row_ptr, dg.col, dg.w, dg.n, dg.m, dg.src, dg.dist, p)
-    return st.kernel_ms, trace_read(device)
+    p = _dc.replace(schedule_params(base, lead, rest, level), trace=True)
+    sssp_device(dg.row_ptr, dg.col, dg.w, dg.n, dg.m, dg.src, dg.dist, p)
+    return trace_read(device)
 
 
-def config_params(base, delta: int, level: int):
-    import dataclasses as _dc
-    return _dc.replace(base, delta=delta, level=level)
-
-
-def _spread(c, p0, p1, dt):
-    """Add an iteration's time dt to the progress bins its span [p0, p1) overlaps,
-    in proportion to the overlap; a span without progress charges its own bin."""
-    nb = len(PROGRESS_BINS) - 1
-    if p1 <= p0 + 1e-12:
-        b = int(np.searchsorted(PROGRESS_BINS, p0, side="right") - 1)
-        c[min(max(b, 0), nb - 1)] += dt
-        return
-    lo = np.maximum(PROGRESS_BINS[:-1], p0)
-    hi = np.minimum(PROGRESS_BINS[1:], p1)
-    c += dt * np.clip(hi - lo, 0.0, None) / (p1 - p0)
-
-
-def label_graph(runs):
-    """runs: {(delta_idx, level_idx): (ms, records)} for one graph.
-    Returns X [R, 12], yd [R], yl [R], wt [R] over all records of all runs."""
-    final = max(recs[-1]["reached"] for _, recs in runs.values() if recs)
-    nb = len(PROGRESS_BINS) - 1
-    cost = {}
-    rows = []
-    for cfg, (ms, recs) in runs.items():
-        c = np.zeros(nb)
-        prev_t = 0.0
-        prev_p = 0.0
-        for r in recs:
-            p1 = r["reached"] / max(final, 1)
-            _spread(c, prev_p, p1, r["t_us"] - prev_t)
-            prev_t = r["t_us"]
-            prev_p = p1
-            # the decision taken after this record shapes the iterations that start here
-            b = min(max(int(np.searchsorted(PROGRESS_BINS, p1, side="right") - 1), 0), nb - 1)
-            rows.append((cfg, b, r["feat"]))
-        cost[cfg] = c
-    cfgs = list(cost)
-    C = np.stack([cost[k] for k in cfgs])  # [configs, bins]
-    best = C.argmin(axis=0)
-    gain = np.median(C, axis=0) - C.min(axis=0)
-    X, yd, yl, wt = [], [], [], []
-    for cfg, b, feat in rows:
-        d_i, l_i = cfgs[best[b]]
-        X.append(feat)
-        yd.append(d_i)
-        yl.append(l_i)
-        wt.append(gain[b] + 1e-3)
-    return (np.array(X, np.float32), np.array(yd, np.int64), np.array(yl, np.int64), np.array(wt, np.float32))
+def label_trace(recs, n: int, lead, level: int, weight: float = 1.0):
+    """X [R+1, 12], yd [R+1] (-1 where no bucket decision follows), yl, wt."""
+    X = [start_features(n)]
+    yd = [int(lead[0])]
+    for i, r in enumerate(recs):
+        X.append(np.asarray(r["feat"], np.float32))
+        nxt = recs[i + 1] if i + 1 < len(recs) else None
+        if nxt is not None and (nxt["level"] & 0x200) and nxt["delta"] > 0:
+            yd.append(int(np.log2(nxt["delta"])))
+        else:
+            yd.append(-1)
+    R = len(X)
+    return (np.stack(X).astype(np.float32), np.array(yd, np.int64), np.full(R, level, np.int64),
+            np.full(R, weight, np.float32))
 
 
 def train(X, yd, yl, wt, device, steps: int = 1500, lr: float = 3e-3, seed: int = 0, log_every: int = 0):

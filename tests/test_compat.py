@@ -1,0 +1,47 @@
+"""The drop-in `void sssp_np_consolidate_gpu(void)` shim linked the way a
+reference build would link it: a harness owns the reference's globals and
+fills them as prepare_gpu() does (tests/compat/harness.cpp).  On CPU the shim
+and harness compile and link against libnps for every CONSOLIDATE_LEVEL; on
+the GPU the harness runs and its distances hash to the oracle's."""
+import os
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "nested-parallelism_b200")
+CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+
+
+def _build(out, level):
+    cmd = ["g++", "-O2", "-std=c++17", f"-DCONSOLIDATE_LEVEL={level}", "-I", os.path.join(ROOT, "include"),
+           "-I", os.path.join(CUDA, "include"), os.path.join(ROOT, "tests", "compat", "harness.cpp"),
+           os.path.join(PKG, "compat", "sssp_np_consolidate_gpu.cpp"), "-o", str(out), "-L", PKG, "-lnps",
+           "-L", os.path.join(CUDA, "lib64"), "-lcudart", f"-Wl,-rpath,{PKG}:{os.path.join(CUDA, 'lib64')}"]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    return str(out)
+
+
+@pytest.fixture(scope="module")
+def harnesses(tmp_path_factory):
+    d = tmp_path_factory.mktemp("compat")
+    return {lv: _build(d / f"harness_l{lv}", lv) for lv in (0, 1, 2)}
+
+
+def test_shim_builds_against_reference_globals(harnesses):
+    for path in harnesses.values():
+        assert os.access(path, os.X_OK)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("level", [0, 1, 2])
+@pytest.mark.parametrize("kind,size,seed", [("uniform", 16384, 1), ("rmat", 14, 5)])
+def test_shim_matches_the_oracle(nps, oracle, cuda_device, harnesses, level, kind, size, seed):
+    r = subprocess.run([harnesses[level], kind, str(size), str(seed)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    f = dict(zip(r.stdout.split()[0::2], r.stdout.split()[1::2]))
+    g = nps.gen_rmat(size, 16, seed=seed) if kind == "rmat" else nps.gen_uniform(size, 8 * size, 100, seed)
+    ref = oracle.sssp_heap(g.row_ptr, g.col, g.w, g.source)
+    assert int(f["status"]) == 0 and int(f["source"]) == g.source
+    assert int(f["fnv1a"], 16) == nps.fnv1a(ref)
+    assert int(f["update_left"]) == 0 and int(f["iterations"]) > 0

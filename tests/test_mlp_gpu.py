@@ -98,3 +98,28 @@ def test_fused_policy_takes_the_oracle_decisions(nps, pol, cuda_device):
         x = ((np.array(a["feat"], np.float64) - w.mean) * w.istd)[None, :]
         _, o = M.forward(w.w1, w.b1, w.w2, w.b2, x.astype(np.float32))
         assert (b["level"] & 0xFF) == int(o[0, 11:].argmax())
+
+
+def test_fused_policy_widths_follow_the_oracle(nps, pol, cuda_device):
+    """The first bucket's width comes from the start-state features and every
+    advance's width from the features of the iteration before it."""
+    g = nps.gen_rmat(14, 16, seed=21)
+    w = pol.MLPWeights.init(17)
+    w.b2[:11] = np.linspace(0.0, 0.5, 11)  # spread the width logits
+    pol.load_into_kernel(w, 0)
+    p = nps.Params(policy=nps.POLICY_LEARNED, trace=True, light_heavy=False)
+    d, st = nps.sssp(g, g.source, p)
+    tr = nps.trace_read(0)
+
+    def k_of(feat):
+        x = ((np.asarray(feat, np.float64) - w.mean) * w.istd)[None, :]
+        _, o = M.forward(w.w1, w.b1, w.w2, w.b2, x.astype(np.float32))
+        return int(o[0, :11].argmax())
+
+    assert tr[0]["delta"] == 1 << k_of(pol.start_features(g.n))
+    adv = 0
+    for a, b in zip(tr[:-1], tr[1:]):
+        if b["level"] & 0x200:
+            assert b["delta"] == 1 << k_of(a["feat"])
+            adv += 1
+    assert adv == st.buckets

@@ -291,3 +291,23 @@ def test_grid_tier_small_threshold_items(nps, oracle, cuda_device, rmat16, unifo
     for g in (rmat16, uniform):
         for delta in (0, 50):
             _check(nps, oracle, g, g.source, _p(nps, level=2, threshold=1, delta=delta))
+
+
+@pytest.mark.parametrize("first,rest", [([2], 10), ([1, 1], 6), ([0, 3, 5, 2, 7, 1, 9], 4), ([], 1)])
+@pytest.mark.parametrize("lh", [False, True])
+def test_delta_schedule(nps, oracle, cuda_device, rmat16, grid128, first, rest, lh):
+    """Per-bucket widths from Params.delta_schedule (the form a learned policy's
+    decisions take): every schedule gives the oracle's distances."""
+    word = nps.delta_schedule(first, rest)
+    for g in (rmat16, grid128):
+        st = _check(nps, oracle, g, g.source, _p(nps, level=2, delta_schedule=word, light_heavy=lh, threshold=32))
+        assert st.buckets > 0
+
+
+def test_delta_schedule_word():
+    import importlib
+    nps = importlib.import_module("nested-parallelism_b200")
+    assert nps.delta_schedule([2], 10) == 0xAAAAAAA2
+    assert nps.delta_schedule([], 3) == 0x33333333
+    with pytest.raises(ValueError):
+        nps.delta_schedule([16], 1)
