@@ -530,6 +530,7 @@ struct Smem {
   uint32_t red[4][BS / 32];
   float feat[NPS_MLP_IN];
   float hid[NPS_MLP_HID];
+  float logit[NPS_MLP_OUT];
   int32_t pol_choice[2];
   TeamDesc team;
   int32_t team_id;
@@ -662,8 +663,14 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
         s = e = 0;
       }
       acc.processed++;
-      if (want_hist) atomicAdd(&sm.hist[deg_bin(e - s)], 1u);
     }
+  }
+  if (want_hist) {
+    // frontier degree histogram: one shared atomic per distinct bin in the warp
+    const bool has = v >= 0;
+    const int bin = has ? deg_bin(e - s) : 8;
+    const uint32_t grp = __match_any_sync(kFull, bin);
+    if (has && lane == __ffs(grp) - 1) atomicAdd(&sm.hist[bin], (uint32_t)__popc(grp));
   }
   if (advance) {
     const bool f[1] = {repush};
@@ -692,21 +699,33 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
     if (slot < (uint32_t)kBlockListCap) sm.blk[slot] = make_int4(s, e, vtag, (int32_t)(uint32_t)old);
     else wtier = true;  // CTA list full: the warp walks the row itself
   }
-  if (gtier) {
-    const uint32_t nch = row_chunks(s, e);
-    const unsigned long long old = atomicAdd(C.heavy_ctr, (1ull << kHeavyShift) | nch);
-    const uint32_t slot = (uint32_t)(old >> kHeavyShift);
-    const uint32_t off = (uint32_t)(old & kHeavyMask);
-    if (slot < C.hcap) {
-      C.heavy[slot] = make_int4(s, e, vtag, (int32_t)off);
-      // this entry holds the first chunk of every work item that starts inside it
-      const uint32_t sh = I.item_shift;
-      for (uint32_t b = (off + (1u << sh) - 1) >> sh; (b << sh) < off + nch; ++b) {
-        if (b < I.icap) C.hitem[b] = (int32_t)slot;
-        else atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_CAPACITY);
+  {
+    uint32_t slot = 0xffffffffu, b0 = 0, b1 = 0;  // list slot and work items [b0, b1) starting in it
+    if (gtier) {
+      const uint32_t nch = row_chunks(s, e);
+      const unsigned long long old = atomicAdd(C.heavy_ctr, (1ull << kHeavyShift) | nch);
+      const uint32_t off = (uint32_t)(old & kHeavyMask);
+      slot = (uint32_t)(old >> kHeavyShift);
+      if (slot < C.hcap) {
+        C.heavy[slot] = make_int4(s, e, vtag, (int32_t)off);
+        const uint32_t sh = I.item_shift;
+        b0 = (off + (1u << sh) - 1) >> sh;
+        b1 = ((off + nch - 1) >> sh) + 1;
+        if (b1 > I.icap) atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_CAPACITY);
+      } else {
+        atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_CAPACITY);
       }
-    } else {
-      atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_CAPACITY);
+    }
+    // the entry holds the first chunk of every work item that starts inside it; the
+    // warp writes those item starts together, one appended row at a time
+    uint32_t wb = __ballot_sync(kFull, b1 > b0);
+    while (wb) {
+      const int src_lane = __ffs(wb) - 1;
+      wb &= wb - 1;
+      const uint32_t rs = __shfl_sync(kFull, slot, src_lane);
+      const uint32_t r0 = __shfl_sync(kFull, b0, src_lane);
+      const uint32_t r1 = min(__shfl_sync(kFull, b1, src_lane), I.icap);
+      for (uint32_t b = r0 + lane; b < r1; b += 32) C.hitem[b] = (int32_t)rs;
     }
   }
 
@@ -882,13 +901,15 @@ __device__ __noinline__ void policy_eval(const PolicyDev* pol, Smem<BS>& sm) {
     sm.hid[t] = a > 0.f ? a : 0.f;
   }
   __syncthreads();
+  if (t < NPS_MLP_OUT) {
+    float a = pol->b2[t];
+#pragma unroll
+    for (int h = 0; h < NPS_MLP_HID; ++h) a = fmaf(bf16_bits_to_float(pol->w2[t * NPS_MLP_HID + h]), sm.hid[h], a);
+    sm.logit[t] = a;
+  }
+  __syncthreads();
   if (t == 0) {
-    float lg[NPS_MLP_OUT];
-    for (int o = 0; o < NPS_MLP_OUT; ++o) {
-      float a = pol->b2[o];
-      for (int h = 0; h < NPS_MLP_HID; ++h) a = fmaf(bf16_bits_to_float(pol->w2[o * NPS_MLP_HID + h]), sm.hid[h], a);
-      lg[o] = a;
-    }
+    const float* lg = sm.logit;
     int bd = 0;
     for (int o = 1; o < 11; ++o)
       if (lg[o] > lg[bd]) bd = o;
