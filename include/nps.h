@@ -69,7 +69,8 @@ enum {
 
 enum {
   NPS_POLICY_PLAIN = 0,    /* fixed delta and level from nps_params */
-  NPS_POLICY_LEARNED = 1   /* per-iteration delta / level from the MLP policy loaded with nps_policy_set_weights */
+  NPS_POLICY_LEARNED = 1   /* bucket widths (first from the start state, then at each advance) and the level of
+                              every iteration from the MLP loaded with nps_policy_set_weights; error if none */
 };
 
 typedef struct nps_params {
