@@ -635,7 +635,8 @@ __device__ __forceinline__ void warp_row(const InstDesc& I, const IterCtx& C, in
 template <int BS>
 __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const IterCtx& C, Smem<BS>& sm,
                                                     int32_t vin, bool advance, uint32_t T_old, bool want_hist,
-                                                    Acc& acc, Stage& S, PhaseClock& pc, int lane) {
+                                                    Acc& acc, Stage& S, PhaseClock& pc, int lane,
+                                                    bool local = false) {
   int32_t v = vin, s = 0, e = 0;
   uint32_t du = 0;
   bool repush = false;
@@ -689,9 +690,11 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
   // deferred entries remember which edges they relax in the top bit of the vertex id
   const int32_t vtag = C.heavy_iter ? (int32_t)((uint32_t)v | 0x80000000u) : v;
   const bool small = deg > 0 && deg < C.t_warp;
-  bool wtier = deg >= C.t_warp && deg < C.t_block;
-  const bool btier = deg >= C.t_block && deg < C.t_grid;
-  const bool gtier = deg >= C.t_grid && deg > 0;
+  // A vertex taken back by a warp-local round is walked by that warp: the CTA and grid
+  // lists then hold each vertex at most once per iteration, which bounds their size.
+  bool wtier = local ? deg >= C.t_warp : (deg >= C.t_warp && deg < C.t_block);
+  const bool btier = !local && deg >= C.t_block && deg < C.t_grid;
+  const bool gtier = !local && deg >= C.t_grid && deg > 0;
   if (btier) {
     // slot and chunk offset from one atomic, so offsets increase with the slot
     const unsigned long long old = atomicAdd(&sm.blk_ctr, (1ull << 32) | row_chunks(s, e));
@@ -1069,7 +1072,12 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     const int32_t* srcq = advance ? I.fq[ep & 1] : (heavy_it ? I.sq[hg & 1] : I.q[it & 1]);
     const uint32_t srclen = advance ? adv_len : (heavy_it ? slen : qlen);
     const uint32_t n_heavy_items = (uint32_t)((hprev_tot + (1ull << I.item_shift) - 1) >> I.item_shift);
-    const uint32_t n_items = n_heavy_items + (srclen + 31) / 32;
+    // vertex items hold 32 frontier entries, or 16 / 8 / 4 when the frontier is small
+    // against the team's warps: a small frontier's rows then spread over more warps
+    // instead of leaving a few warps with 32 rows each
+    uint32_t vper = 32;
+    while (vper > 4 && (unsigned long long)srclen < (unsigned long long)vper * team_size * NW) vper >>= 1;
+    const uint32_t n_items = n_heavy_items + (srclen + vper - 1) / vper;
     Acc acc = {0, 0, 0, 0};
     Stage S;
     S.nbuf = sm.stage[warp][0];
@@ -1125,9 +1133,9 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
           walk_item(I, C, Hprev, hprev_cnt, kb, ke, (uint32_t)js, acc, S, lane);
           NPS_LAP(pc, 4);
         } else {
-          const uint32_t idx = (uint32_t)(item - n_heavy_items) * 32 + lane;
-          process_vertex_item<BS>(I, C, sm, idx < srclen ? srcq[idx] : -1, advance, T_old, want_iter, acc, S,
-                                  pc, lane);
+          const uint32_t idx = (uint32_t)(item - n_heavy_items) * vper + lane;
+          process_vertex_item<BS>(I, C, sm, ((uint32_t)lane < vper && idx < srclen) ? srcq[idx] : -1, advance,
+                                  T_old, want_iter, acc, S, pc, lane);
           // warp-local rounds: vertices this warp just queued for the next iteration are
           // taken back from its staging buffer and processed now, up to local_rounds times;
           // their stamp is reset so a later improvement in this iteration queues them again
@@ -1141,7 +1149,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
             }
             __syncwarp();
             S.ncnt -= k;
-            process_vertex_item<BS>(I, C, sm, lv, false, T_old, want_iter, acc, S, pc, lane);
+            process_vertex_item<BS>(I, C, sm, lv, false, T_old, want_iter, acc, S, pc, lane, true);
           }
         }
       }
