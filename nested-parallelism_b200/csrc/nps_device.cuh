@@ -236,18 +236,21 @@ __device__ __forceinline__ int deg_bin(int32_t d) {
   return b > 7 ? 7 : b;
 }
 
-// Distance read for the pre-check `nd < dist[v]` before atomicMin: L2 only (the
-// value must be current), with the evict-last policy.
+// Distance read for the pre-check `nd < dist[v]` before atomicMin: cached in L1
+// (`.ca`) with the L2 evict-last policy.  An L1 copy may be stale, but within a
+// launch distances only decrease, and L1 lines of global data do not survive
+// from one launch to the next (PTX ISA, ld cache operators: the driver
+// invalidates them between dependent grids), so a stale value is never below
+// the current one: the pre-check can only let an extra candidate through to the
+// atomicMin, whose returned old value decides.  On R-MAT graphs
+// the heads of most edges are a few thousand hub vertices; serving their
+// distances from L1 takes that load off a handful of L2 slices.
 __device__ __forceinline__ uint32_t ld_dist(const uint32_t* p) {
-#if defined(NPS_DIST_L1)
-  uint32_t v;
-  asm volatile("ld.global.ca.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(policy_evict_last()));
-  return v;
-#elif defined(NPS_NO_L2_HINTS)
-  return __ldcg(p);
+#ifdef NPS_NO_L2_HINTS
+  return __ldca(p);
 #else
   uint32_t v;
-  asm volatile("ld.global.cg.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(policy_evict_last()));
+  asm volatile("ld.global.ca.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(policy_evict_last()));
   return v;
 #endif
 }
