@@ -199,7 +199,7 @@ def run_reference(a, nps, g, m_r, n_r, cfg):
     times = [r[0] for r in res]
     value = a.steps * m_r / wall / 1e9
     line = {
-        "impl": "reference", "metric": "sssp_gteps", "value": value, "unit": "GTEPS", "n_gpus": a.gpus,
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": a.gpus,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * statistics.mean(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic", "config": cfg,

@@ -110,7 +110,8 @@ typedef struct nps_stats {
   uint32_t reached;         /* vertices with a finite distance */
   uint32_t pad0;
   uint64_t reached_edges;   /* out-edges of reached vertices (m_r) */
-  float kernel_ms;          /* device time of the persistent launch (CUDA events) */
+  float kernel_ms;          /* device time of the persistent launch (CUDA events); per instance of a
+                               batch: device time from the launch to the end of that instance's solve */
   float total_ms;           /* device time including copies done by the call */
   int32_t status;           /* device status word */
   int32_t grid_ctas;        /* CTAs in the persistent launch */

@@ -82,7 +82,8 @@ struct __align__(128) Counters {
   uint32_t it_reached[3];
   uint32_t pad1[3];
   unsigned long long prof[9];   // NPS_PROFILE builds: SM cycles per phase, summed over warps
-  unsigned long long pad2[7];
+  unsigned long long solve_ns;  // end of this instance's solve, from its team CTA 0's start
+  unsigned long long pad2[6];
   // striped work counters, one 128-byte line each: work[slot][stripe * 32]
   uint32_t work[3][kStripes * 32];
 };
@@ -532,9 +533,8 @@ struct Smem {
   int32_t stage[BS / 32][3][kStage];  // per-warp append staging: [near, far, settle]
   uint32_t red[4][BS / 32];
   float feat[NPS_MLP_IN];
-  float hid[NPS_MLP_HID];
-  float logit[NPS_MLP_OUT];
   int32_t pol_choice[2];
+  uint32_t it_acc[3];          // this CTA's edges, improvements, first reaches in the iteration
   TeamDesc team;
   int32_t team_id;
   uint32_t rank;
@@ -557,9 +557,18 @@ constexpr uint32_t kBarGroup = 16;  // barrier-area sizing granule (words per te
 template <int BS>
 __device__ __forceinline__ bool team_barrier(const LaunchParams& P, Smem<BS>& sm, uint32_t* bar,
                                              uint32_t& epoch, uint32_t team_size,
-                                             uint32_t* status, bool inject, bool check_status = true) {
+                                             uint32_t* status, bool inject, bool check_status = true,
+                                             Counters* flush = nullptr, uint32_t flush_slot = 0) {
   __syncthreads();
   if (threadIdx.x == 0) {
+    if (flush) {
+      // this CTA's iteration statistics, ordered before the arrival by the release
+      if (sm.it_acc[0]) atomicAdd(&flush->it_edges[flush_slot], (unsigned long long)sm.it_acc[0]);
+      if (sm.it_acc[1]) atomicAdd(&flush->it_impr[flush_slot], (unsigned long long)sm.it_acc[1]);
+      if (sm.it_acc[2]) atomicAdd(&flush->it_reached[flush_slot], sm.it_acc[2]);
+      for (int b = 0; b < 8; ++b)
+        if (sm.hist[b]) atomicAdd(&flush->hist[flush_slot][b], sm.hist[b]);
+    }
     if (globaltimer_ns() - sm.t_start > P.run_budget_ns) {
       atomicCAS(status, 0u, (uint32_t)NPS_ERR_TIMEOUT);
       atomicExch(P.abort_flag, 1u);
@@ -896,36 +905,40 @@ __device__ __forceinline__ float bf16_bits_to_float(uint16_t b) {
   return __uint_as_float(((uint32_t)b) << 16);
 }
 
-template <int BS>
-__device__ __noinline__ void policy_eval(const PolicyDev* pol, Smem<BS>& sm) {
-  const int t = threadIdx.x;
-  __syncthreads();
-  if (t < NPS_MLP_HID) {
-    float a = pol->b1[t];
+// One warp evaluates the MLP on the normalised features in shared memory: lane h
+// computes hidden unit h, lanes 0..13 the logits (the hidden layer reaches them
+// by shuffles), then two shuffle arg-max reductions (lowest index on ties) give
+// the width exponent (logits 0..10) and the level (logits 11..13), written to
+// choice[0] and choice[1].  Called by all 32 lanes of one warp.
+static __device__ __noinline__ void policy_eval_warp(const PolicyDev* pol, const float* feat, int32_t* choice, int lane) {
+  static_assert(NPS_MLP_HID == 32 && NPS_MLP_OUT <= 32, "one lane per hidden unit and per logit");
+  float a = pol->b1[lane];
 #pragma unroll
-    for (int i = 0; i < NPS_MLP_IN; ++i) a = fmaf(bf16_bits_to_float(pol->w1[t * NPS_MLP_IN + i]), sm.feat[i], a);
-    sm.hid[t] = a > 0.f ? a : 0.f;
-  }
-  __syncthreads();
-  if (t < NPS_MLP_OUT) {
-    float a = pol->b2[t];
+  for (int i = 0; i < NPS_MLP_IN; ++i) a = fmaf(bf16_bits_to_float(pol->w1[lane * NPS_MLP_IN + i]), feat[i], a);
+  const float hid = a > 0.f ? a : 0.f;
+  const int o = lane < NPS_MLP_OUT ? lane : 0;
+  float lg = pol->b2[o];
 #pragma unroll
-    for (int h = 0; h < NPS_MLP_HID; ++h) a = fmaf(bf16_bits_to_float(pol->w2[t * NPS_MLP_HID + h]), sm.hid[h], a);
-    sm.logit[t] = a;
+  for (int h = 0; h < NPS_MLP_HID; ++h)
+    lg = fmaf(bf16_bits_to_float(pol->w2[o * NPS_MLP_HID + h]), __shfl_sync(kFull, hid, h), lg);
+  // arg-max over [lo, hi): the larger value wins, the lower index on equal values
+  auto argmax = [&](int lo, int hi) {
+    float v = (lane >= lo && lane < hi) ? lg : -INFINITY;
+    int ix = (lane >= lo && lane < hi) ? lane : 0x7fffffff;
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) {
+      const float v2 = __shfl_xor_sync(kFull, v, d);
+      const int i2 = __shfl_xor_sync(kFull, ix, d);
+      if (v2 > v || (v2 == v && i2 < ix)) { v = v2; ix = i2; }
+    }
+    return ix;
+  };
+  const int bd = argmax(0, 11);
+  const int bl = argmax(11, NPS_MLP_OUT) - 11;
+  if (lane == 0) {
+    choice[0] = bd;
+    choice[1] = bl;
   }
-  __syncthreads();
-  if (t == 0) {
-    const float* lg = sm.logit;
-    int bd = 0;
-    for (int o = 1; o < 11; ++o)
-      if (lg[o] > lg[bd]) bd = o;
-    int bl = 0;
-    for (int o = 1; o < 3; ++o)
-      if (lg[11 + o] > lg[11 + bl]) bl = o;
-    sm.pol_choice[0] = bd;
-    sm.pol_choice[1] = bl;
-  }
-  __syncthreads();
 }
 
 // Tier thresholds (warp, block, grid) for a consolidation level.
@@ -996,16 +1009,31 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
   int level = I.level;
   if (learned) {
     // the first bucket's width and the first level come from the policy too, on the
-    // start state: log2(1 + frontier), no degree histogram, no advances, 1 of n reached
+    // start state.  The first bucket is filled by the source's out-neighbours, so a
+    // single-source start reports that frontier: log2(1 + out-degree of the source)
+    // and the source's degree bin; the state form reports its initial frontier size
+    // and no histogram.  No advances, 1 of n reached.
     if (threadIdx.x == 0) {
+      int sbin = -1;
+      float f0 = log2f(1.f + (float)qlen);
+      if (I.mode == 0 && qlen == 1) {
+        const int32_t sd = __ldg(I.row_ptr + I.src + 1) - __ldg(I.row_ptr + I.src);
+        sbin = deg_bin(sd);
+        f0 = log2f(1.f + (float)sd);
+      }
       for (int i = 0; i < NPS_MLP_IN; ++i) {
         float f = 0.f;
-        if (i == 0) f = log2f(1.f + (float)qlen);
+        if (i == 0) f = f0;
+        if (i >= 1 && i <= 8 && i - 1 == sbin) f = 1.f;
         if (i == 10) f = 1.f / (float)I.n;
         sm.feat[i] = (f - P.policy->mean[i]) * P.policy->istd[i];
       }
     }
-    policy_eval<BS>(P.policy, sm);
+    if (warp == 0) {
+      __syncwarp();
+      policy_eval_warp(P.policy, sm.feat, sm.pol_choice, lane);
+    }
+    __syncthreads();
     delta = 1u << sm.pol_choice[0];
     level = sm.pol_choice[1];
   }
@@ -1070,6 +1098,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
       }
     }
     if (threadIdx.x < 8) sm.hist[threadIdx.x] = 0;
+    if (threadIdx.x < 3) sm.it_acc[threadIdx.x] = 0;
     __syncthreads();
 
     const int32_t* srcq = advance ? I.fq[ep & 1] : (heavy_it ? I.sq[hg & 1] : I.q[it & 1]);
@@ -1176,17 +1205,17 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     stage_drain(S, C, I.qcap, &ctr->status, lane);
     NPS_LAP(pc, 6);
 
-    // ---- per-CTA flush of iteration counters
+    // ---- iteration counters (policy features, trace): warp sums into shared
+    // memory; thread 0 adds the CTA's totals to the instance counters just before
+    // it arrives at the barrier, so the release orders them before the arrival
     if (want_iter) {
-      uint32_t r[4];
-      block_sum4<BS>(sm, acc.edges, acc.impr, acc.reached, acc.processed, r);
-      if (threadIdx.x == 0) {
-        const uint32_t sl = it % 3;
-        if (r[0]) atomicAdd(&ctr->it_edges[sl], (unsigned long long)r[0]);
-        if (r[1]) atomicAdd(&ctr->it_impr[sl], (unsigned long long)r[1]);
-        if (r[2]) atomicAdd(&ctr->it_reached[sl], r[2]);
-        for (int b = 0; b < 8; ++b)
-          if (sm.hist[b]) atomicAdd(&ctr->hist[sl][b], sm.hist[b]);
+      const uint32_t e = __reduce_add_sync(kFull, acc.edges);
+      const uint32_t im = __reduce_add_sync(kFull, acc.impr);
+      const uint32_t rc = __reduce_add_sync(kFull, acc.reached);
+      if (lane == 0) {
+        if (e) atomicAdd(&sm.it_acc[0], e);
+        if (im) atomicAdd(&sm.it_acc[1], im);
+        if (rc) atomicAdd(&sm.it_acc[2], rc);
       }
     }
     tot.edges += acc.edges;
@@ -1195,7 +1224,9 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     tot.processed += acc.processed;
 
     NPS_LAP(pc, 8);
-    if (!team_barrier<BS>(P, sm, bar, bar_epoch, team_size, &ctr->status, false, false)) return;
+    if (!team_barrier<BS>(P, sm, bar, bar_epoch, team_size, &ctr->status, false, false,
+                          want_iter ? ctr : nullptr, it % 3))
+      return;
     NPS_LAP(pc, 7);
 
     // ---- decide the next iteration (every CTA reads the same values)
@@ -1204,17 +1235,78 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
       buckets += 1;
     }
     if (heavy_it) hg += 1;
-    // thread 0 reads the shared counters and the status word once per CTA and broadcasts them
+    // thread 0 reads the shared counters, the status word and (for the policy or
+    // the trace) this iteration's statistics in one batch of loads, and
+    // broadcasts them; with the learned policy, warp 0 then evaluates the MLP on
+    // the features thread 0 computed (every CTA reads the same counters, so every
+    // CTA takes the same decision)
     if (threadIdx.x == 0) {
-      sm.bc_q = __ldcg(&ctr->qtail[(it + 1) % 3]);
-      sm.bc_h = ld_relaxed_u64(&ctr->heavy[it % 3]);
-      sm.bc_f = __ldcg(&ctr->ftail[ep % 3]);
-      sm.bc_m = __ldcg(&ctr->fmin[ep % 3]);
-      sm.bc_s = __ldcg(&ctr->stail[hg % 3]);
-      if (ld_relaxed_u32(&ctr->status) != 0) {
+      const uint32_t sl = it % 3;
+      const uint32_t q1 = __ldcg(&ctr->qtail[(it + 1) % 3]);
+      const unsigned long long h1 = ld_relaxed_u64(&ctr->heavy[it % 3]);
+      const uint32_t f1 = __ldcg(&ctr->ftail[ep % 3]);
+      const uint32_t m1 = __ldcg(&ctr->fmin[ep % 3]);
+      const uint32_t s1 = __ldcg(&ctr->stail[hg % 3]);
+      const uint32_t st1 = ld_relaxed_u32(&ctr->status);
+      uint32_t hb[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      unsigned long long ie = 0, ii = 0;
+      uint32_t ir = 0;
+      if (want_iter) {
+        for (int b = 0; b < 8; ++b) hb[b] = __ldcg(&ctr->hist[sl][b]);
+        ie = __ldcg(&ctr->it_edges[sl]);
+        ii = __ldcg(&ctr->it_impr[sl]);
+        ir = __ldcg(&ctr->it_reached[sl]);
+      }
+      sm.bc_q = q1;
+      sm.bc_h = h1;
+      sm.bc_f = f1;
+      sm.bc_m = m1;
+      sm.bc_s = s1;
+      if (st1 != 0) {
         atomicExch(P.abort_flag, 1u);
         sm.ok = 0;
       }
+      if (want_iter) {
+        // The 12 policy features: log2 of the next frontier, the out-degree histogram
+        // of this iteration's frontier as 8 fractions, log2(1 + bucket advances), the
+        // reached fraction, improvements per scanned edge.
+        reached_total += ir;
+        const uint32_t qn0 = min(q1, I.qcap);
+        const uint32_t fl0 = min(f1, I.qcap);
+        const uint32_t hn0 = min((uint32_t)(h1 >> kHeavyShift), hhalf);
+        const bool adv0 = qn0 == 0 && hn0 == 0 && fl0 != 0;
+        float hs = 0.f;
+        for (int b = 0; b < 8; ++b) hs += (float)hb[b];
+        const float inv = hs > 0.f ? 1.f / hs : 0.f;
+        float f[NPS_MLP_IN];
+        f[0] = log2f(1.f + (float)(adv0 ? fl0 : qn0));
+        for (int b = 0; b < 8; ++b) f[1 + b] = (float)hb[b] * inv;
+        f[9] = log2f(1.f + (float)buckets);
+        f[10] = (float)reached_total / (float)I.n;
+        f[11] = ie ? (float)ii / (float)ie : 0.f;
+        if (learned)
+          for (int i = 0; i < NPS_MLP_IN; ++i) sm.feat[i] = (f[i] - P.policy->mean[i]) * P.policy->istd[i];
+        if (I.trace && rank == 0 && it < I.trace_cap) {
+          nps_trace_rec* tr = I.trace + it;
+          tr->iteration = it;
+          tr->frontier = srclen;
+          tr->far_len = fl0;
+          tr->bucket_hi = T;
+          tr->delta = delta;
+          tr->level = (uint32_t)level | (heavy_it ? 0x100u : 0u) | (advance ? 0x200u : 0u);
+          for (int b = 0; b < 8; ++b) tr->hist[b] = hb[b];
+          tr->edges = ie;
+          tr->improvements = ii;
+          tr->reached = reached_total;
+          tr->heavy = hn0;
+          tr->t_ns = globaltimer_ns() - sm.t_start;
+          for (int i = 0; i < NPS_MLP_IN; ++i) tr->feat[i] = f[i];
+        }
+      }
+    }
+    if (learned && warp == 0) {
+      __syncwarp();
+      if (sm.ok) policy_eval_warp(P.policy, sm.feat, sm.pol_choice, lane);
     }
     __syncthreads();
     if (!sm.ok) return;
@@ -1222,51 +1314,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     const unsigned long long hc = sm.bc_h;
     const uint32_t hn = min((uint32_t)(hc >> kHeavyShift), hhalf);
     const uint32_t fl = min(sm.bc_f, I.qcap);
-    const bool will_advance = qn == 0 && hn == 0 && fl != 0;
-
-    if (want_iter) {
-      const uint32_t sl = it % 3;
-      reached_total += __ldcg(&ctr->it_reached[sl]);
-      const int level_used = level;
-      // The 12 policy features, computed by thread 0 of every CTA from the same
-      // counters (so every CTA takes the same decision): log2 of the next frontier,
-      // the out-degree histogram of this iteration's frontier as 8 fractions,
-      // log2(1 + bucket advances), the reached fraction, improvements per scanned edge.
-      if (threadIdx.x == 0) {
-        float h[8], hs = 0.f;
-        for (int b = 0; b < 8; ++b) { h[b] = (float)__ldcg(&ctr->hist[sl][b]); hs += h[b]; }
-        const float inv = hs > 0.f ? 1.f / hs : 0.f;
-        float f[NPS_MLP_IN];
-        f[0] = log2f(1.f + (float)(will_advance ? fl : qn));
-        for (int b = 0; b < 8; ++b) f[1 + b] = h[b] * inv;
-        f[9] = log2f(1.f + (float)buckets);
-        f[10] = (float)reached_total / (float)I.n;
-        const unsigned long long ie = __ldcg(&ctr->it_edges[sl]);
-        f[11] = ie ? (float)__ldcg(&ctr->it_impr[sl]) / (float)ie : 0.f;
-        if (learned)
-          for (int i = 0; i < NPS_MLP_IN; ++i) sm.feat[i] = (f[i] - P.policy->mean[i]) * P.policy->istd[i];
-        if (I.trace && rank == 0 && it < I.trace_cap) {
-          nps_trace_rec* tr = I.trace + it;
-          tr->iteration = it;
-          tr->frontier = srclen;
-          tr->far_len = fl;
-          tr->bucket_hi = T;
-          tr->delta = delta;
-          tr->level = (uint32_t)level_used | (heavy_it ? 0x100u : 0u) | (advance ? 0x200u : 0u);
-          for (int b = 0; b < 8; ++b) tr->hist[b] = __ldcg(&ctr->hist[sl][b]);
-          tr->edges = ie;
-          tr->improvements = __ldcg(&ctr->it_impr[sl]);
-          tr->reached = reached_total;
-          tr->heavy = hn;
-          tr->t_ns = globaltimer_ns() - sm.t_start;
-          for (int i = 0; i < NPS_MLP_IN; ++i) tr->feat[i] = f[i];
-        }
-      }
-      if (learned) {
-        policy_eval<BS>(P.policy, sm);
-        level = sm.pol_choice[1];
-      }
-    }
+    if (learned) level = sm.pol_choice[1];
 
     hprev_cnt = hn;
     hprev_tot = hc & kHeavyMask;
@@ -1319,6 +1367,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
   if (threadIdx.x == 0) {
     if (rank == 0) {
       ctr->iterations = it;
+      ctr->solve_ns = globaltimer_ns() - sm.t_start;
       ctr->buckets = buckets;
       *I.stamp_base = base + (it > ep ? it : ep) + 4;
     }

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <queue>
 #include <set>
 #include <string>
 #include <vector>
@@ -723,7 +724,7 @@ extern "C" nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, co
     ctl.base = c->b_control.p;
 
     // team formation: longest-processing-time assignment of instances to
-    // nteams teams by work (m + n), then CTAs proportional to team work
+    // nteams teams by work (m + n), then CTAs by water-filling on work per CTA
     std::vector<int> idx(count);
     for (int i = 0; i < count; ++i) idx[i] = i;
     auto work = [&](int i) { return (double)inst[i].m + (double)inst[i].n; };
@@ -735,21 +736,20 @@ extern "C" nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, co
       tw[t] += work(i);
       members[t].push_back(i);
     }
-    double total = 0;
-    for (double x : tw) total += x;
+    // CTAs: one per team, then each further CTA to the team with the most work per
+    // CTA (minimises the largest work / CTAs ratio over integer CTA counts)
     std::vector<int> ctas(nteams, 1);
-    int left = grid - nteams;
-    std::vector<std::pair<double, int>> frac;
-    for (int t = 0; t < nteams; ++t) {
-      double want = total > 0 ? (double)(grid)*tw[t] / total : (double)grid / nteams;
-      int extra = std::max(0, (int)std::floor(want) - 1);
-      extra = std::min(extra, left);
-      ctas[t] += extra;
-      left -= extra;
-      frac.push_back({want - std::floor(want), t});
+    {
+      using Q = std::pair<double, int>;
+      std::priority_queue<Q> pq;
+      for (int t = 0; t < nteams; ++t) pq.push({tw[t], t});
+      for (int left = grid - nteams; left > 0; --left) {
+        const int t = pq.top().second;
+        pq.pop();
+        ctas[t] += 1;
+        pq.push({tw[t] / ctas[t], t});
+      }
     }
-    std::sort(frac.begin(), frac.end(), [](auto& a, auto& b) { return a.first > b.first; });
-    for (size_t k = 0; left > 0 && k < frac.size(); ++k, --left) ctas[frac[k].second]++;
     std::vector<TeamDesc> teams(nteams);
     std::vector<int32_t> order;
     int cb = 0;
@@ -872,6 +872,7 @@ extern "C" nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, co
       fill_stats(k, &per_instance[i]);
       per_instance[i].reached = k.reached + 1;
       per_instance[i].grid_ctas = grid;
+      per_instance[i].kernel_ms = (float)((double)k.solve_ns * 1e-6);  // device time to this instance's end
     }
     if (k.status && !first_err) first_err = k.status;
   }

@@ -181,9 +181,10 @@ REST_K = (8, 10)           # log2 width of every later bucket
 
 def candidate_schedules(max_lead: int = 4):
     """(leading exponents, rest exponent) pairs: non-decreasing leading widths,
-    1..max_lead of them, then a wide remainder."""
+    1..max_lead of them, then a wide remainder; plus the wide width from the
+    start (the plain kernel's unordered behaviour on these graphs)."""
     import itertools
-    out = []
+    out = [((r,), r) for r in REST_K]
     for n in range(1, max_lead + 1):
         for lead in itertools.combinations_with_replacement(LEADING_K, n):
             for r in REST_K:
@@ -220,10 +221,21 @@ def teacher_search(dg, base, schedules, reps: int = 3):
     return lv_ms[level], best, level, times
 
 
-def start_features(n: int, frontier: int = 1) -> np.ndarray:
-    """The start-state features the kernel evaluates before its first iteration."""
+def degree_bin(d: int) -> int:
+    """Out-degree bin of the frontier histogram: [4^k - 1, 4^(k+1) - 1), last bin open."""
+    return min(((int(d) + 1).bit_length() - 1) >> 1, 7)
+
+
+def start_features(n: int, source_degree: int = None, frontier: int = 1) -> np.ndarray:
+    """The start-state features the kernel evaluates before its first iteration.
+    A single-source start reports the frontier that fills the first bucket, the
+    source's out-neighbours: log2(1 + out-degree) and the source's degree bin; a
+    start from a state reports log2(1 + frontier) and no histogram.  1/n reached."""
     f = np.zeros(IN, np.float32)
     f[0] = np.log2(1.0 + frontier)
+    if source_degree is not None and frontier == 1:
+        f[0] = np.log2(1.0 + int(source_degree))
+        f[1 + degree_bin(int(source_degree))] = 1.0
     f[10] = 1.0 / n
     return f
 
@@ -237,9 +249,9 @@ def trace_schedule(dg, base, lead, rest, level, device: int = 0):
     return trace_read(device)
 
 
-def label_trace(recs, n: int, lead, level: int, weight: float = 1.0):
+def label_trace(recs, n: int, lead, level: int, weight: float = 1.0, source_degree: int = None):
     """X [R+1, 12], yd [R+1] (-1 where no bucket decision follows), yl, wt."""
-    X = [start_features(n)]
+    X = [start_features(n, source_degree)]
     yd = [int(lead[0])]
     for i, r in enumerate(recs):
         X.append(np.asarray(r["feat"], np.float32))

@@ -91,7 +91,8 @@ def main():
                     wins[s] += 1
             p_ms = pol._time(dg, plain)
             recs = pol.trace_schedule(dg, base, lead, rest, level)
-            X, yd, yl, wt = pol.label_trace(recs, g.n, lead, level)
+            X, yd, yl, wt = pol.label_trace(recs, g.n, lead, level,
+                                            source_degree=int(g.row_ptr[g.source + 1] - g.row_ptr[g.source]))
             Xs.append(X); yds.append(yd); yls.append(yl); wts.append(wt)
             rows.append({"scale": scale, "seed": seed, "plain_ms": p_ms, "teacher_ms": best_ms,
                          "lead": list(lead), "rest": rest, "level": level, "records": int(len(X))})

@@ -116,7 +116,7 @@ def test_fused_policy_widths_follow_the_oracle(nps, pol, cuda_device):
         _, o = M.forward(w.w1, w.b1, w.w2, w.b2, x.astype(np.float32))
         return int(o[0, :11].argmax())
 
-    assert tr[0]["delta"] == 1 << k_of(pol.start_features(g.n))
+    assert tr[0]["delta"] == 1 << k_of(pol.start_features(g.n, int(g.row_ptr[g.source + 1] - g.row_ptr[g.source])))
     adv = 0
     for a, b in zip(tr[:-1], tr[1:]):
         if b["level"] & 0x200:
