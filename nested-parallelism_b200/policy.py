@@ -4,7 +4,7 @@ A 2-layer MLP (12 features -> 32 ReLU -> 14 logits; bf16 weights, fp32
 accumulation) picks the width delta = 2^k (k = 0..10) of the first bucket
 (from the start state) and of every bucket a bucket advance opens, and, at
 every iteration, the consolidation level (warp / block / grid).  Inference runs inside the persistent kernel
-(policy_eval in csrc/nps_device.cuh); training runs on the GPU through the
+(policy_eval_warp in csrc/nps_device.cuh); training runs on the GPU through the
 forward / loss-backward / Adam kernels of csrc/nps_mlp.cu.  Device memory is
 plain torch tensors; all arithmetic is in those kernels.
 
