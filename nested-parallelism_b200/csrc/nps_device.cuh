@@ -416,7 +416,12 @@ __device__ __forceinline__ void append_k(int32_t* q, uint32_t* tail, uint32_t ca
 // vertices it pushes and moves them to the global queue 32 at a time (one
 // atomicAdd on the queue tail per >= 32 entries, one coalesced 128-byte store
 // per 32), so warps do not serialise on the tail counter every round.
-constexpr int kStage = 160;  // >= 31 left over + 4 * 32 from one append
+// A warp moves its staged appends to the global queue once kFlushAt are waiting,
+// in multiples of 32, with one atomicAdd on the queue tail: fewer, larger flushes
+// keep the single tail counter of each queue from serialising the improvements
+// of a large iteration.
+constexpr int kFlushAt = 64;
+constexpr int kStage = kFlushAt + 4 * 32;  // >= kFlushAt - 1 left over + 4 * 32 from one append
 
 struct Stage {
   int32_t* nbuf;   // near-queue staging (kStage entries, shared memory)
@@ -466,7 +471,7 @@ __device__ __forceinline__ void stage_k(int32_t* buf, uint32_t& cnt, const bool 
     base += __popc(b[j]);
   }
   cnt += tot;
-  if (cnt >= 32) stage_flush(buf, cnt, cnt & ~31u, q, tail, cap, status, lane);
+  if (cnt >= (uint32_t)kFlushAt) stage_flush(buf, cnt, cnt & ~31u, q, tail, cap, status, lane);
 }
 
 // End of an iteration: everything staged goes to the global queues.
