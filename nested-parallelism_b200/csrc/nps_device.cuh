@@ -376,9 +376,18 @@ __device__ __forceinline__ void relax_batch(const InstDesc& I, const IterCtx& C,
         pn[j] = atomicExch(I.mark + v[j], C.snear) != C.snear;
       } else {
         pf[j] = atomicExch(I.fmark + v[j], C.sfar) != C.sfar;
-        if (pf[j] && C.fp_min) atomicMin(C.fp_min, nd[j]);
       }
     }
+  }
+  if (C.fp_min) {
+    // smallest distance pushed into the far pile: one atomicMin per warp (all lanes
+    // take part; a single per-push atomic on this one word serialises an advance)
+    uint32_t mn = 0xffffffffu;
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+      if (pf[j]) mn = min(mn, nd[j]);
+    mn = __reduce_min_sync(kFull, mn);
+    if ((threadIdx.x & 31) == 0 && mn != 0xffffffffu) atomicMin(C.fp_min, mn);
   }
 }
 
@@ -667,7 +676,6 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
       } else if (du >= C.T) {
         if (__ldcg(I.fmark + v) != C.sfar) {
           repush = atomicExch(I.fmark + v, C.sfar) != C.sfar;
-          if (repush) atomicMin(C.fp_min, du);
         }
         rv = v;
         v = -1;
@@ -691,6 +699,8 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
     if (has && lane == __ffs(grp) - 1) atomicAdd(&sm.hist[bin], (uint32_t)__popc(grp));
   }
   if (advance) {
+    const uint32_t mn = __reduce_min_sync(kFull, repush ? du : 0xffffffffu);
+    if (lane == 0 && mn != 0xffffffffu) atomicMin(C.fp_min, mn);
     const bool f[1] = {repush};
     const int32_t vv[1] = {rv};
     stage_k<1>(S.fbuf, S.fcnt, f, vv, C.fp, C.fp_tail, I.qcap, &I.ctr->status, lane);
@@ -721,12 +731,29 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
   }
   {
     uint32_t slot = 0xffffffffu, b0 = 0, b1 = 0;  // list slot and work items [b0, b1) starting in it
-    if (gtier) {
-      const uint32_t nch = row_chunks(s, e);
-      const unsigned long long old = atomicAdd(C.heavy_ctr, (1ull << kHeavyShift) | nch);
-      const uint32_t off = (uint32_t)(old & kHeavyMask);
-      slot = (uint32_t)(old >> kHeavyShift);
-      if (slot < C.hcap) {
+    // one atomicAdd per warp reserves list slots and chunk offsets for all of its
+    // grid-tier rows (a per-row atomic on this one counter serialises large frontiers);
+    // within the warp, slots and offsets follow lane order, so offsets still grow
+    // with the slot across the list
+    const uint32_t gmask = __ballot_sync(kFull, gtier);
+    if (gmask) {
+      const uint32_t nch = gtier ? row_chunks(s, e) : 0u;
+      uint32_t incl = nch;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+      }
+      const uint32_t wtot = __shfl_sync(kFull, incl, 31);
+      const int leader = __ffs(gmask) - 1;
+      unsigned long long old = 0;
+      if (lane == leader) old = atomicAdd(C.heavy_ctr, ((unsigned long long)__popc(gmask) << kHeavyShift) | wtot);
+      old = __shfl_sync(kFull, old, leader);
+      const uint32_t off = (uint32_t)(old & kHeavyMask) + (incl - nch);
+      slot = (uint32_t)(old >> kHeavyShift) + (uint32_t)__popc(gmask & lanemask_lt());
+      if (!gtier) {
+        slot = 0xffffffffu;
+      } else if (slot < C.hcap) {
         C.heavy[slot] = make_int4(s, e, vtag, (int32_t)off);
         const uint32_t sh = I.item_shift;
         b0 = (off + (1u << sh) - 1) >> sh;
