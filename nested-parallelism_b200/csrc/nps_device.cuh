@@ -57,7 +57,6 @@ constexpr uint32_t kInf = NPS_INF;
 constexpr int kHeavyShift = 36;  // heavy counter packs (count << 36) | chunk_offset
 constexpr unsigned long long kHeavyMask = (1ull << kHeavyShift) - 1;
 constexpr int kStripes = 8;            // striped work counters
-constexpr int kHeavyItemShift = 6;     // at least 2^6 chunks (256 edges) per grid-tier work item
 constexpr int kBlockListCap = 512;     // CTA list entries (block tier)
 
 // Per-instance device counters.  Zeroed by the host before a launch.
@@ -105,7 +104,7 @@ struct InstDesc {
   int4* heavy;          // grid-tier entries {row start, row end, vertex | heavy flag, chunk offset}
   int32_t* hitem;       // per half: entry holding the first chunk of each grid-tier work item
   uint32_t icap;        // work items per half
-  uint32_t item_shift;  // log2 chunks per grid-tier work item (>= kHeavyItemShift)
+  uint32_t item_shift;  // log2 chunks per grid-tier work item (5 or more)
   int32_t* sq[2];       // settle lists (light/heavy split): vertices processed in the bucket
   uint32_t* smark;      // settle-list dedupe stamps
   uint32_t qcap;
