@@ -223,6 +223,14 @@ __device__ __forceinline__ int32_t ld_stream(const int32_t* p) {
   return v;
 }
 
+// Read-only index data (row_ptr) read once per visit: no L1 allocation, so L1
+// keeps the distance lines.
+__device__ __forceinline__ int32_t ld_index(const int32_t* p) {
+  int32_t v;
+  asm volatile("ld.global.nc.L1::no_allocate.s32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+
 __device__ __forceinline__ uint32_t lanemask_lt() {
   uint32_t m;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -592,7 +600,10 @@ __device__ __forceinline__ bool team_barrier(const LaunchParams& P, Smem<BS>& sm
     const unsigned long long t0 = globaltimer_ns();
     int ok = 1;
     uint32_t spins = 0;
-    while ((int32_t)(ld_acquire_u32(bar) - target) < 0) {
+    // Spin with relaxed loads and acquire once the count is reached: an acquire
+    // at GPU scope makes the SM drop its L1 copies of global data, which would
+    // also throw away the distance lines the SM's other CTAs are still using.
+    while ((int32_t)(ld_relaxed_u32(bar) - target) < 0) {
       if ((++spins & 15u) == 0) {
         if (ld_relaxed_u32(P.abort_flag)) { ok = 0; break; }
         if (globaltimer_ns() - t0 > P.timeout_ns) {
@@ -604,6 +615,7 @@ __device__ __forceinline__ bool team_barrier(const LaunchParams& P, Smem<BS>& sm
       }
       __nanosleep(20);
     }
+    if (ok) (void)ld_acquire_u32(bar);  // synchronises with every arrival's release
     if (ok && check_status && ld_relaxed_u32(status) != 0) ok = 0;
     if (!ok) atomicExch(P.abort_flag, 1u);
     sm.ok = ok;
@@ -681,8 +693,8 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
       }
     }
     if (v >= 0) {
-      s = __ldg(I.row_ptr + v);
-      e = __ldg(I.row_ptr + v + 1);
+      s = ld_index(I.row_ptr + v);
+      e = ld_index(I.row_ptr + v + 1);
       if (s < 0 || e < s || e > I.m) {  // malformed CSR row: record and skip
         atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_FORMAT);
         s = e = 0;
@@ -894,7 +906,7 @@ __device__ __forceinline__ void walk_item(const InstDesc& I, const IterCtx& C, c
     int4 E = make_int4(0, 0, 0, 0);
     uint32_t off = 0xffffffffu, cov = 0xffffffffu, dv = kInf;
     if (jl < cnt) {
-      E = L[jl];
+      E = __ldcg(L + jl);  // written last iteration; read at L2, not kept in L1
       off = (uint32_t)E.w;
       cov = off + row_chunks(E.x, E.y);
       const uint32_t v = (uint32_t)E.z & 0x7fffffffu;
@@ -1197,7 +1209,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
           NPS_LAP(pc, 4);
         } else {
           const uint32_t idx = (uint32_t)(item - n_heavy_items) * vper + lane;
-          process_vertex_item<BS>(I, C, sm, ((uint32_t)lane < vper && idx < srclen) ? srcq[idx] : -1, advance,
+          process_vertex_item<BS>(I, C, sm, ((uint32_t)lane < vper && idx < srclen) ? __ldcg(srcq + idx) : -1, advance,
                                   T_old, want_iter, acc, S, pc, lane);
           // warp-local rounds: vertices this warp just queued for the next iteration are
           // taken back from its staging buffer and processed now, up to local_rounds times;
