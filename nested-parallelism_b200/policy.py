@@ -209,15 +209,24 @@ def _time(dg, params, reps: int = 3) -> float:
     return float(np.median(ts))
 
 
+LEVEL_MARGIN = 0.05  # another level must beat the plain configuration's by 5 % to become the label
+
+
 def teacher_search(dg, base, schedules, reps: int = 3):
     """Fastest (schedule, level) for one device graph.  Returns
-    (best_ms, (lead, rest), level, {schedule: ms})."""
+    (best_ms, (lead, rest), level, {schedule: ms}).  The level label stays the plain
+    configuration's unless another level is faster by LEVEL_MARGIN: level timings
+    within a few percent are noise, and labels that flip between them teach the
+    network nothing."""
     times = {}
     for lead, rest in schedules:
         times[(lead, rest)] = _time(dg, schedule_params(base, lead, rest), reps)
     best = min(times, key=times.get)
     lv_ms = {lv: _time(dg, schedule_params(base, best[0], best[1], lv), reps) for lv in LEVEL_CHOICES}
-    level = min(lv_ms, key=lv_ms.get)
+    level = base.level if base.level in lv_ms else min(lv_ms, key=lv_ms.get)
+    fastest = min(lv_ms, key=lv_ms.get)
+    if lv_ms[fastest] < (1.0 - LEVEL_MARGIN) * lv_ms[level]:
+        level = fastest
     return lv_ms[level], best, level, times
 
 
