@@ -3,8 +3,9 @@
 A 2-layer MLP (12 features -> 32 ReLU -> 14 logits; bf16 weights, fp32
 accumulation) picks the width delta = 2^k (k = 0..10) of the first bucket
 (from the start state) and of every bucket a bucket advance opens, and, at
-every iteration, the consolidation level (warp / block / grid).  Inference runs inside the persistent kernel
-(policy_eval_warp in csrc/nps_device.cuh); training runs on the GPU through the
+every iteration, the consolidation level (warp / block / grid).  Inference runs
+inside the persistent kernel (policy_eval_warp in csrc/nps_device.cuh); training
+runs on the GPU through the
 forward / loss-backward / Adam kernels of csrc/nps_mlp.cu.  Device memory is
 plain torch tensors; all arithmetic is in those kernels.
 
@@ -16,8 +17,9 @@ The 12 features (computed in-kernel after each iteration's barrier):
   11     improvements per scanned edge in the iteration
 
 Delta-stepping is exact for any delta and any level, so the policy changes only
-speed; the plain kernel remains the fallback (no weights loaded, or
-Params.policy = POLICY_PLAIN) and distances are identical either way.
+speed; the plain kernel (Params.policy = POLICY_PLAIN, the default) remains the
+fallback and the judge, and distances are identical either way.  A learned call
+on a device without weights loaded is an error, not a silent fallback.
 """
 from __future__ import annotations
 
