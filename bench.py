@@ -10,8 +10,9 @@ source = highest-out-degree vertex.  One step = one full SSSP from that source.
   plain    the autotuner picks fixed parameters on this graph (outside the timed
            region); K steps of that configuration are timed first
   value    GTEPS = m_r / kernel time (m_r = out-edges of reached vertices) of the
-           learned-policy kernel (nested-parallelism_b200/policy_weights.npz; the
-           plain parameters with the MLP choosing bucket widths and levels); graph
+           learned-policy kernel (nested-parallelism_b200/policy_weights.npz; the MLP
+           chooses bucket widths and levels, a short autotune of its own picks the
+           degree threshold and block shape); graph
            resident in HBM, L2 flushed between steps, CUDA events on the launch stream
   e2e      the same metric through the public host-buffer call nps.sssp(): pinned
            host CSR -> device, kernel, distances -> host, every step
@@ -61,6 +62,8 @@ WORKLOADS = {
 }
 
 METRIC = "SSSP GTEPS on 1 B200: learned-policy vs plain, % of HBM roofline, bit-exact"
+LEARNED_AXES = {"threshold": [16, 32, 64, 128], "block_size": [256, 512]}
+LEARNED_TUNE_BUDGET = 8
 
 # autotuner seed configuration per workload class (--delta / --level pin it instead)
 DEFAULT_PARAMS = {
@@ -483,6 +486,13 @@ def main():
         pol.load_into_kernel(pol.MLPWeights.load(wpath), local)
         learned = dataclasses.replace(plain, policy=nps.POLICY_LEARNED, light_heavy=False, order_degree=0,
                                       delta_schedule=0)
+        if tune_log:
+            # the learned arm's static parameters (degree threshold, block shape) get their
+            # own short autotune; the policy itself picks widths and levels
+            learned, _, ltune = at.autotune([dg], repeats=3, budget=LEARNED_TUNE_BUDGET, seed=learned,
+                                            axes=LEARNED_AXES)
+            learned.device = local
+            tune_log = tune_log + ltune
     params = learned if use_learned else plain
 
     flush = torch.empty(256 << 20, dtype=torch.int8, device=dev)  # > 126 MB L2
