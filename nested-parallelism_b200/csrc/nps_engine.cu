@@ -258,6 +258,14 @@ struct nps_ctx {
   int b_grid = 0, b_bs = 0;
   int b_nteams = 0;
   cudaGraphExec_t b_graph = nullptr;
+  // Re-balancing of the teams of an unchanged instance set (one instance per team):
+  // stage 0 splits CTAs by work; the solve times of the first two calls (taken with
+  // different splits) calibrate a per-team model, after which the split is fixed.
+  int b_stage = 0;
+  std::vector<int> b_inst_ctas;   // CTAs of each instance's team in the current split
+  std::vector<double> b_t1, b_t2; // measured solve times (ms) of the first two calls
+  std::vector<int> b_c1, b_c2;    // ... and their teams' CTAs
+  std::vector<uint32_t> b_it1;    // iterations in the first call
   Counters* h_ctr = nullptr;  // pinned
   size_t h_ctr_n = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -692,10 +700,15 @@ extern "C" nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, co
   int grid = 0;
   if ((e = grid_size(c->device, c->di, p.block_size, false, p.ctas_per_sm, &grid))) return e;
 
-  const bool same = c->b_graph && (int)c->b_key.size() == count && c->b_grid == grid && c->b_bs == p.block_size &&
-                    memcmp(c->b_key.data(), inst, sizeof(nps_instance) * count) == 0 &&
-                    memcmp(&c->b_params_key, &p, sizeof(p)) == 0;
+  const bool same_set = (int)c->b_key.size() == count && c->b_grid == grid && c->b_bs == p.block_size &&
+                        memcmp(c->b_key.data(), inst, sizeof(nps_instance) * count) == 0 &&
+                        memcmp(&c->b_params_key, &p, sizeof(p)) == 0;
   const int nteams = std::min(count, grid);
+  if (!same_set || nteams != count) c->b_stage = 0;
+  // stages 1 and 2 form the teams anew (a captured graph is captured again); stage 3
+  // keeps the last split
+  const bool rebalance = c->b_stage == 1 || c->b_stage == 2;
+  const bool same = same_set && c->b_graph && !rebalance;
   Control ctl((size_t)count, (size_t)nteams, grid);
 
   if (!same) {
@@ -736,20 +749,49 @@ extern "C" nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, co
       tw[t] += work(i);
       members[t].push_back(i);
     }
-    // CTAs: one per team, then each further CTA to the team with the most work per
-    // CTA (minimises the largest work / CTAs ratio over integer CTA counts)
+    // CTAs: one per team, then each further CTA to the team whose predicted time is
+    // largest.  The prediction is a + b / CTAs per team:
+    //   stage 0   a = 0, b = work (m + n): minimises the largest work / CTAs ratio;
+    //   stage 1   from the first call's solve time T1 with c1 CTAs: a = iterations x
+    //             kIterFloorMs (the latency floor more CTAs do not shorten),
+    //             b = (T1 - a) x c1;
+    //   stage 2+  fitted through the first two calls' (c1, T1) and (c2, T2).
+    constexpr double kIterFloorMs = 0.008;
+    std::vector<double> fa(nteams, 0.0), fb(nteams, 0.0);
+    for (int t = 0; t < nteams; ++t) {
+      if (c->b_stage == 0) {
+        fb[t] = tw[t];
+        continue;
+      }
+      const int i = members[t][0];
+      const double t1 = c->b_t1[i], c1 = std::max(c->b_c1[i], 1);
+      fa[t] = c->b_it1[i] * kIterFloorMs;
+      fb[t] = std::max(t1 - fa[t], 0.05 * t1) * c1;
+      if (c->b_stage >= 2 && c->b_c2[i] != c->b_c1[i]) {
+        const double t2 = c->b_t2[i], c2 = std::max(c->b_c2[i], 1);
+        const double b = (t1 - t2) / (1.0 / c1 - 1.0 / c2);
+        const double a = t1 - b / c1;
+        if (b > 0 && a >= 0) {
+          fa[t] = a;
+          fb[t] = b;
+        }
+      }
+    }
     std::vector<int> ctas(nteams, 1);
     {
       using Q = std::pair<double, int>;
       std::priority_queue<Q> pq;
-      for (int t = 0; t < nteams; ++t) pq.push({tw[t], t});
+      for (int t = 0; t < nteams; ++t) pq.push({fa[t] + fb[t], t});
       for (int left = grid - nteams; left > 0; --left) {
         const int t = pq.top().second;
         pq.pop();
         ctas[t] += 1;
-        pq.push({tw[t] / ctas[t], t});
+        pq.push({fa[t] + fb[t] / ctas[t], t});
       }
     }
+    c->b_inst_ctas.assign(count, 0);
+    for (int t = 0; t < nteams; ++t)
+      for (int i : members[t]) c->b_inst_ctas[i] = ctas[t];
     std::vector<TeamDesc> teams(nteams);
     std::vector<int32_t> order;
     int cb = 0;
@@ -876,6 +918,19 @@ extern "C" nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, co
     }
     if (k.status && !first_err) first_err = k.status;
   }
+  if (!first_err && nteams == count && c->b_stage < 2) {
+    std::vector<double>& t = c->b_stage == 0 ? c->b_t1 : c->b_t2;
+    t.resize(count);
+    for (int i = 0; i < count; ++i) t[i] = (double)c->h_ctr[i].solve_ns * 1e-6;
+    if (c->b_stage == 0) {
+      c->b_it1.resize(count);
+      for (int i = 0; i < count; ++i) c->b_it1[i] = c->h_ctr[i].iterations;
+      c->b_c1 = c->b_inst_ctas;
+    } else {
+      c->b_c2 = c->b_inst_ctas;
+    }
+  }
+  if (!first_err && nteams == count && c->b_stage < 3) c->b_stage += 1;
   if (first_err) {  // stamps of an aborted batch may collide with the next run's
     cudaMemsetAsync(c->b_stamp.p, 0, c->b_stamp.n * sizeof(uint32_t), s);
     cudaStreamSynchronize(s);
