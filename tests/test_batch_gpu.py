@@ -51,3 +51,20 @@ def test_device_batch_results_match_the_oracle(nps, cuda_device, batch64, want):
     for r, ref, st in zip(res, want[:20], stats):
         assert r["fnv1a"] == nps.fnv1a(ref)
         assert r["reached"] == int((ref < nps.INF).sum()) == st.reached
+
+
+def test_rebalanced_batch_stays_exact(nps, cuda_device, batch64, want):
+    """Calls 2 and 3 on an unchanged instance set re-balance the teams' CTAs from the
+    measured per-instance solve times (and re-capture the graph); every call, before
+    and after, gives the oracle's distances, and each instance reports its solve time."""
+    B = importlib.import_module("nested-parallelism_b200.batch")
+    db = B.DeviceBatch(batch64, cuda_device)
+    p = nps.Params(level=2, threshold=64, delta=0, block_size=512)
+    for call in range(5):
+        for k in db.keep:
+            k[3].fill_(-1)
+        stats, ms = db.run(p, use_graph=True)
+        assert ms > 0
+        assert all(st.status == 0 and st.kernel_ms > 0 for st in stats)
+        for got, ref in zip(db.distances(), want):
+            assert np.array_equal(got, ref), f"call {call}"
