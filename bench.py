@@ -56,6 +56,9 @@ WORKLOADS = {
                  "4096x4096 4-neighbour grid, 5% pairs dropped, w in [1,1000], seed 1, source (0,0)"),
     "uniform16k": ("uniform", dict(n=16384, m=131072, wmax=100, seed=1),
                    "uniform random 16,384 vertices / 131,072 edges, w in [1,100], seed 1, source 0"),
+    "degree22": ("degree", dict(scale=22, edge_factor=16, seed=1000),
+                 "degree statistics (the reference's graph analyzer) of R-MAT scale 22, edge factor 16, "
+                 "seed 1000: extremes, totals, 8-bin histogram and full distribution"),
     "batch64": ("batch", dict(count=64, seed=7),
                 "64 R-MAT instances (a=.57 b=.19 c=.19), scale U{12..18}, edge factor {4,8,16,32}, "
                 "w in [1,255], random sources, seed 7; one persistent CUDA-graph launch per shard"),
@@ -416,6 +419,73 @@ def bench_batch(a, nps, ws, rank, local, desc):
     return 0
 
 
+def bench_degree(a, nps, ws, rank, local, desc):
+    """Degree statistics of the R-MAT scale-22 graph through nps_degree_stats on device
+    row offsets (two streaming passes: statistics, then the distribution).  value =
+    bytes of row offsets streamed per second; each call is synchronous, so the time
+    includes the two launches and the host round trips."""
+    _, args, _ = WORKLOADS[a.workload]
+    g = nps.gen_rmat(args["scale"], args["edge_factor"], seed=args["seed"])
+    cfg = {"workload": a.workload, "description": desc, "n": g.n, "m": g.m}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if a.impl == "reference":
+        if rank == 0:
+            times = []
+            for _ in range(a.warmup):
+                oracle.degree_stats(g.row_ptr)
+            for _ in range(a.steps):
+                _, t = oracle.timed(oracle.degree_stats, g.row_ptr)
+                times.append(t)
+            bytes_ = 8 * (g.n + 1)
+            value = bytes_ * a.steps / sum(times) / 1e9
+            print(json.dumps({"impl": "reference", "metric": "degree_stats_gbs", "value": value, "unit": "GB/s",
+                              "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+                              "ms_per_step": 1e3 * sum(times) / a.steps, "higher_is_better": True,
+                              "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+                              "config": cfg,
+                              "cpu_baseline": {"value": value, "unit": "GB/s", "cores": 1, "kind": "port",
+                                               "sample": "the oracle's numpy restatement of getStatInfo()"},
+                              "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}))
+        return 0
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    row = torch.from_numpy(g.row_ptr.view(np.int32)).to(dev)
+    want = oracle.degree_stats(g.row_ptr)
+    for _ in range(a.warmup):
+        st = nps.degree_stats(row, device=local)
+    exact = bool(np.array_equal(st["dist"], want["dist"]) and st["max_degree_node"] == want["max_degree_node"])
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        st = nps.degree_stats(row, device=local)
+    dt = (time.perf_counter() - t0) / a.steps
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        nps.degree_stats(g, device=local)
+    dt_e2e = (time.perf_counter() - t0) / a.steps
+    bytes_ = 8 * (g.n + 1)  # row offsets, read by both passes
+    peak, peak_src = load_peaks()
+    if rank == 0:
+        cpu = None
+        if not a.no_cpu_baseline:
+            _, tcpu = oracle.timed(oracle.degree_stats, g.row_ptr)
+            cpu = {"value": bytes_ / tcpu / 1e9, "unit": "GB/s", "cores": 1, "kind": "port",
+                   "sample": "one run of the oracle's numpy restatement of getStatInfo() on the same graph"}
+        print(json.dumps({"metric": "degree_stats_gbs", "value": bytes_ / dt / 1e9, "unit": "GB/s", "n_gpus": ws,
+                          "steps": a.steps, "warmup": a.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+                          "config": dict(cfg, exact_vs_oracle=exact, timing="host wall clock per synchronous call"),
+                          "roofline": {"bound": "hbm", "achieved": bytes_ / dt / 1e9, "peak": peak, "unit": "GB/s",
+                                       "frac": bytes_ / dt / 1e9 / peak, "traffic": None, "peak_source": peak_src},
+                          "e2e": {"value": bytes_ / dt_e2e / 1e9, "unit": "GB/s", "h2d_bytes_per_step": 4 * (g.n + 1),
+                                  "d2h_bytes_per_step": 8 * (st["max_degree"] + 1), "ms_per_step": dt_e2e * 1e3},
+                          "gpu_launches": 2 * a.steps, "cpu_baseline": cpu}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -437,6 +507,8 @@ def main():
     kind, _, desc = WORKLOADS[a.workload]
     if kind == "batch":
         return bench_batch(a, nps, ws, rank, local, desc)
+    if kind == "degree":
+        return bench_degree(a, nps, ws, rank, local, desc)
     prm = dict(DEFAULT_PARAMS[kind])
     if a.delta is not None:
         prm["delta"] = a.delta

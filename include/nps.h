@@ -247,6 +247,32 @@ typedef struct nps_instance {
 nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, const nps_params* p,
                           int32_t use_graph, nps_stats* per_instance, float* kernel_ms);
 
+/* ---- degree statistics ----------------------------------------------------
+ * The reference's graph analyzer (utility/graph-analyzer/analyzer.cpp:75-138,
+ * getStatInfo()) on the GPU, from the CSR row offsets: counts, total / average /
+ * maximum / minimum out-degree with the lowest vertex id attaining each, and
+ * optionally the degree distribution.  The minimum starts from the reference's
+ * 999999 (a graph whose degrees are all at least that reports 999999 and node -1).
+ * Also the 8-bin histogram [4^k - 1, 4^(k+1) - 1) of the policy's features. */
+typedef struct nps_degree_info {
+  int32_t n;                /* noNodeTotal */
+  int32_t max_degree;
+  int64_t m;                /* row_ptr[n] (noEdgeTotal) */
+  int64_t total_degree;     /* sum of out-degrees */
+  int64_t edges_by_degree;  /* total_degree / 2, the reference's "Edge by degree" */
+  int32_t min_degree;
+  int32_t max_degree_node;  /* lowest id with the maximum degree */
+  int32_t min_degree_node;  /* lowest id with the minimum degree, -1 if none below 999999 */
+  float avg_degree;         /* (float)total_degree / n, as the reference computes it */
+  int64_t bins[8];
+} nps_degree_info;
+/* Synchronous, on the library's own stream of `device`.  dist (dist_len > 0):
+ * vertices per degree 0..dist_len-1 (int64, host or device memory as flagged by
+ * device_ptrs); NPS_ERR_CAPACITY, with info filled, when dist_len <= max_degree.
+ * NPS_ERR_FORMAT when row_ptr decreases. */
+nps_status nps_degree_stats(const int32_t* row_ptr, int32_t n, int32_t device_ptrs, int32_t device,
+                            nps_degree_info* info, int64_t* dist, int64_t dist_len);
+
 /* ---- learned policy (MLP 12 -> 32 -> 14) --------------------------------- */
 #define NPS_MLP_IN 12
 #define NPS_MLP_HID 32

@@ -24,7 +24,7 @@ from typing import Iterable, List, Optional, Sequence
 import numpy as np
 
 from ._native import (NPS_INF, NPS_MLP_HID, NPS_MLP_IN, NPS_MLP_OUT, NpsError, check, lib,
-                      nps_graph, nps_instance, nps_params, nps_stats, nps_trace_rec)
+                      nps_degree_info, nps_graph, nps_instance, nps_params, nps_stats, nps_trace_rec)
 
 INF = NPS_INF
 THRESHOLD = 64
@@ -37,7 +37,7 @@ __all__ = [
     "CONSOLIDATE_HYBRID", "POLICY_PLAIN", "POLICY_LEARNED", "Graph", "Params", "Stats",
     "NpsError", "gen_uniform", "gen_rmat", "gen_grid", "convertCSR", "readInputDIMACS9",
     "readInputDIMACS10", "readInputSLNDC", "writeDIMACS9", "sssp", "sssp_device", "SSSP_GPU",
-    "sssp_np_consolidate_gpu", "sssp_batch", "trace_read", "fnv1a", "delta_schedule", "abi_version", "lib",
+    "sssp_np_consolidate_gpu", "sssp_batch", "trace_read", "fnv1a", "delta_schedule", "degree_stats", "abi_version", "lib",
 ]
 
 
@@ -352,6 +352,41 @@ def sssp_batch(instances: Sequence[Instance], params: Optional[Params] = None, u
     cp = p.to_c(device_ptrs=True, stream=stream)
     check(lib.nps_sssp_batch(arr, k, C.byref(cp), int(bool(use_graph)), stats, C.byref(ms)), "sssp_batch")
     return [Stats.from_c(s) for s in stats], float(ms.value)
+
+
+def degree_stats(g, distribution: bool = True, device: int = 0) -> dict:
+    """Degree statistics of a graph on the GPU: what the reference's graph analyzer
+    prints (utility/graph-analyzer/analyzer.cpp:75-138): Node, Edge, Edge by degree
+    (total / 2), Avg, Max, Min and the lowest node ids with the maximum / minimum
+    degree, plus `bins` (the 8-bin histogram [4^k - 1, 4^(k+1) - 1)) and, with
+    `distribution`, `dist` (vertices per degree, 0..max).  `g` is a Graph or a row
+    offset array (numpy host array, or a device tensor with `data_ptr`)."""
+    if isinstance(g, Graph):
+        row, dev_ptr = np.ascontiguousarray(g.row_ptr, np.int32), False
+    elif hasattr(g, "data_ptr"):
+        row, dev_ptr = g, True
+    else:
+        row, dev_ptr = np.ascontiguousarray(g, np.int32), False
+    n = (int(row.numel()) if dev_ptr else int(row.shape[0])) - 1
+    ptr = row.data_ptr() if dev_ptr else row.ctypes.data
+    info = nps_degree_info()
+    check(lib.nps_degree_stats(ptr, n, int(dev_ptr), device, C.byref(info), None, 0), "degree_stats")
+    out = {"n": info.n, "m": int(info.m), "total_degree": int(info.total_degree),
+           "edges_by_degree": int(info.edges_by_degree), "avg_degree": float(info.avg_degree),
+           "max_degree": info.max_degree, "min_degree": info.min_degree,
+           "max_degree_node": info.max_degree_node, "min_degree_node": info.min_degree_node,
+           "bins": [int(x) for x in info.bins]}
+    if distribution:
+        if dev_ptr:
+            import torch
+            d = torch.empty(info.max_degree + 1, dtype=torch.int64, device=row.device)
+            check(lib.nps_degree_stats(ptr, n, 1, device, C.byref(info), d.data_ptr(), d.numel()), "degree_stats")
+            out["dist"] = d.cpu().numpy()
+        else:
+            d = np.zeros(info.max_degree + 1, np.int64)
+            check(lib.nps_degree_stats(ptr, n, 0, device, C.byref(info), d.ctypes.data, d.shape[0]), "degree_stats")
+            out["dist"] = d
+    return out
 
 
 def trace_read(device: int = 0, cap: int = 1 << 16) -> List[dict]:

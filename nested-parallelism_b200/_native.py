@@ -74,6 +74,14 @@ class nps_instance(C.Structure):
     ]
 
 
+class nps_degree_info(C.Structure):
+    _fields_ = [
+        ("n", C.c_int32), ("max_degree", C.c_int32), ("m", C.c_int64), ("total_degree", C.c_int64),
+        ("edges_by_degree", C.c_int64), ("min_degree", C.c_int32), ("max_degree_node", C.c_int32),
+        ("min_degree_node", C.c_int32), ("avg_degree", C.c_float), ("bins", C.c_int64 * 8),
+    ]
+
+
 _P = C.c_void_p
 _I32, _I64, _U32, _U64, _F, _D = C.c_int32, C.c_int64, C.c_uint32, C.c_uint64, C.c_float, C.c_double
 
@@ -102,6 +110,7 @@ SIGNATURES = {
     "nps_sssp_noalloc": (_I32, [_P, _P, _P, _I32, _I64, _I32, _P, C.POINTER(nps_params), C.POINTER(nps_stats)]),
     "nps_sssp_batch": (_I32, [C.POINTER(nps_instance), _I32, C.POINTER(nps_params), _I32,
                               C.POINTER(nps_stats), C.POINTER(_F)]),
+    "nps_degree_stats": (_I32, [_P, _I32, _I32, _I32, C.POINTER(nps_degree_info), _P, _I64]),
     "nps_policy_set_weights": (_I32, [_I32, _P, _P, _P, _P, _P, _P]),
     "nps_mlp_forward": (_I32, [_P, _P, _P, _P, _P, _I32, _P, _P]),
     "nps_mlp_loss_backward": (_I32, [_P, _P, _P, _P, _P, _P, _P, _P, _I32, _P, _P, _P, _P, _P, _P]),

@@ -162,6 +162,61 @@ def ref_dijkstra_dheap(row, col, w, src, d=2):
     return cost.view(np.uint32), float(t)
 
 
+def degree_stats(row):
+    """Restated getStatInfo() of the reference's graph analyzer
+    (utility/graph-analyzer/analyzer.cpp:75-138) on CSR row offsets: degrees are the
+    row lengths; the maximum and minimum keep the first (lowest) vertex id that
+    attains them, and the minimum starts from 999999 (analyzer.cpp:85-86, strict
+    comparisons at :101-108); the average is float(total) / n (:110); "Edge by
+    degree" is total / 2 (:112).  Also the 8-bin histogram [4^k - 1, 4^(k+1) - 1)
+    and the distribution (vertices per degree, 0..max)."""
+    row = np.ascontiguousarray(row, dtype=np.int64)
+    deg = np.diff(row)
+    n = deg.shape[0]
+    total = int(deg.sum())
+    mx = int(deg.max()) if n else 0
+    below = deg < 999999
+    mn = int(deg[below].min()) if below.any() else 999999
+    lb = np.floor(np.log2(deg.astype(np.float64) + 1.0)).astype(np.int64) >> 1
+    bins = np.bincount(np.minimum(lb, 7), minlength=8)[:8]
+    return {"n": n, "m": int(row[-1]), "total_degree": total, "edges_by_degree": total // 2,
+            "avg_degree": float(np.float32(total) / np.float32(n)), "max_degree": mx, "min_degree": mn,
+            "max_degree_node": int(np.argmax(deg == mx)) if n else -1,
+            "min_degree_node": int(np.argmax(deg == mn)) if below.any() else -1,
+            "bins": [int(x) for x in bins], "dist": np.bincount(deg, minlength=mx + 1).astype(np.int64)}
+
+
+ANALYZER = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_ref", "analyzer")
+
+
+def ref_analyzer(path, fmt=0):
+    """Run the reference's graph analyzer (built from utility/graph-analyzer/ by
+    this directory's Makefile into _ref/analyzer) on a graph file with -d; returns
+    its printed statistics and distribution."""
+    import subprocess
+    r = subprocess.run([ANALYZER, "-i", str(path), "-f", str(int(fmt)), "-d"], capture_output=True, text=True,
+                       timeout=600)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference analyzer failed ({r.returncode}): {r.stderr[-200:]}")
+    out = {"dist": {}}
+    keys = {"Node": "n", "Edge by degree": "edges_by_degree", "Edge": "m", "Avg": "avg_degree",
+            "Max": "max_degree", "Min": "min_degree", "Node ID with max degree": "max_degree_node",
+            "Node ID with min degree": "min_degree_node"}
+    for line in r.stdout.splitlines():
+        if ":" in line:
+            k, v = line.split(":", 1)
+            if k.strip() in keys:
+                out[keys[k.strip()]] = float(v) if k.strip() == "Avg" else int(v)
+        elif line.strip():
+            d, c = line.split()
+            out["dist"][int(d)] = int(c)
+    return out
+
+
+def have_analyzer() -> bool:
+    return os.path.exists(ANALYZER)
+
+
 def timed(fn, *a, **k):
     t0 = time.perf_counter()
     r = fn(*a, **k)

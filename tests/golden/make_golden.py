@@ -4,7 +4,10 @@
 For each case the graph comes from this repository's seeded generators, and the
 expected distances come from the reference's SSSP_CPU() (apps/sssp/src/cpu/
 sssp.cpp:13-47 with common/heap.cpp), compiled from its unmodified sources into
-oracle/_ref/libref_sssp.so by oracle/Makefile.  The reader fixtures are small
+oracle/_ref/libref_sssp.so by oracle/Makefile.  The degree-statistics goldens
+come from the reference's graph analyzer (utility/graph-analyzer/analyzer.cpp),
+built into oracle/_ref/analyzer, run on the reader fixtures and on generated
+graphs written as DIMACS9.  The reader fixtures are small
 synthetic DIMACS9 / DIMACS10 / SNAP files written here; their expected CSR comes
 from the reference's readInputDIMACS9/10/SLNDC() + convertCSR() (common/
 global.cpp:29-235) on the same files.
@@ -99,6 +102,36 @@ def write_reader_fixtures():
             f.write(f"{a}\t{b}\n")
 
 
+# graphs for the degree analyzer: the reader fixtures, and generated graphs written
+# as DIMACS9 for the reference's analyzer to read
+ANALYZER_GRAPHS = [("rmat12_ef8_s9", "rmat", dict(scale=12, edge_factor=8, seed=9)),
+                   ("uniform16k_s1", "uniform", dict(n=16384, m=131072, wmax=100, seed=1)),
+                   ("grid64_s1", "grid", dict(rows=64, cols=64, drop=0.05, wmax=1000, seed=1))]
+
+
+def analyzer_goldens():
+    """The reference's graph analyzer (utility/graph-analyzer/analyzer.cpp, built by
+    oracle/Makefile into oracle/_ref/analyzer) run with -d on each file: its printed
+    statistics and degree distribution."""
+    import tempfile
+    if not oracle.have_analyzer():
+        sys.exit("oracle/_ref/analyzer missing: build it with `make -C oracle` where the reference exists")
+    res = {}
+    for fname, fmt in (("reader_dimacs9.gr", 0), ("reader_dimacs10.graph", 1), ("reader_slndc.txt", 2)):
+        r = oracle.ref_analyzer(os.path.join(HERE, fname), fmt)
+        r["dist"] = sorted([int(k), int(v)] for k, v in r["dist"].items())
+        res[fname] = dict(r, file=fname, format=fmt)
+    with tempfile.TemporaryDirectory() as td:
+        for name, kind, args in ANALYZER_GRAPHS:
+            g = gen(kind, args)
+            path = os.path.join(td, name + ".gr")
+            nps.writeDIMACS9(path, g)
+            r = oracle.ref_analyzer(path, 0)
+            r["dist"] = sorted([int(k), int(v)] for k, v in r["dist"].items())
+            res[name] = dict(r, kind=kind, args=args)
+    return res
+
+
 def main():
     if not oracle.have_reference():
         sys.exit("oracle/_ref/libref_sssp.so missing: build it with `make -C oracle` where the reference exists")
@@ -128,6 +161,7 @@ def main():
         out["readers"][fname] = {"format": fmt, "n": int(row.shape[0] - 1), "m": int(col.shape[0]), "source": src,
                                  "row_fnv1a": nps.fnv1a(row.view(np.uint32)),
                                  "col_fnv1a": nps.fnv1a(col.view(np.uint32)), "w_fnv1a": nps.fnv1a(w)}
+    out["analyzer"] = analyzer_goldens()
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)
     np.savez_compressed(os.path.join(HERE, "golden_dist.npz"), **dists)
