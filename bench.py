@@ -59,6 +59,10 @@ WORKLOADS = {
     "degree22": ("degree", dict(scale=22, edge_factor=16, seed=1000),
                  "degree statistics (the reference's graph analyzer) of R-MAT scale 22, edge factor 16, "
                  "seed 1000: extremes, totals, 8-bin histogram and full distribution"),
+    "solutions22": ("solutions", dict(scale=22, edge_factor=16, seed=1000),
+                    "ablation: SSSP_GPU solutions 0-6 (thread queue, dual queue, shared / global delayed "
+                    "buffer, naive / per-block nested launch, consolidation plain and learned) on R-MAT scale 22, "
+                    "edge factor 16, seed 1000"),
     "batch64": ("batch", dict(count=64, seed=7),
                 "64 R-MAT instances (a=.57 b=.19 c=.19), scale U{12..18}, edge factor {4,8,16,32}, "
                 "w in [1,255], random sources, seed 7; one persistent CUDA-graph launch per shard"),
@@ -486,6 +490,84 @@ def bench_degree(a, nps, ws, rank, local, desc):
     return 0
 
 
+def bench_solutions(a, nps, ws, rank, local, desc):
+    """Every case of SSSP_GPU()'s switch on the R-MAT scale-22 bench graph, device
+    arrays resident, distances checked against the oracle.  Per solution: median
+    device time of the call's iteration loop (CUDA events), GTEPS = reached
+    out-edges / that time, and how much work it did.  value = consolidation with
+    the learned policy (the headline path); the other solutions are the ablation."""
+    _, args, _ = WORKLOADS[a.workload]
+    g = nps.gen_rmat(args["scale"], args["edge_factor"], seed=args["seed"])
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    ref = oracle.sssp_heap(g.row_ptr, g.col, g.w, g.source)
+    n_r, m_r = oracle.reached(g.row_ptr, ref)
+    cfg = {"workload": a.workload, "description": desc, "n": g.n, "m": g.m, "m_reached": m_r, "source": g.source,
+           "threshold": 64, "row_per_thread_cta": 256, "timing": "CUDA events around each call's iteration loop"}
+    if a.impl == "reference":
+        if rank == 0:
+            cfg["parallelism"] = "host cores"
+            print(json.dumps(run_reference(a, nps, g, m_r, n_r, cfg)))
+        return 0
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    at = importlib.import_module("nested-parallelism_b200.autotune")
+    pol = importlib.import_module("nested-parallelism_b200.policy")
+    dg = at.to_device(g, device=dev)
+    reps = max(1, min(a.steps, 3))
+    rows = {}
+
+    def run_solution(sol):
+        stats = []
+        for i in range(1 + reps):  # one untimed call first (workspace, device runtime set-up)
+            d_cost = torch.full((g.n,), nps.INF, dtype=torch.int32, device=dev)
+            d_upd = torch.zeros(g.n, dtype=torch.uint8, device=dev)
+            d_cost[g.source] = 0
+            d_upd[g.source] = 1
+            st, info = nps.sssp_solution_state(sol, dg.row_ptr, dg.col, dg.w, d_cost, d_upd, g.n, g.m,
+                                               nps.Params(device=local, threshold=64, block_size=256))
+            if i:
+                stats.append((st, info))
+        exact = bool((d_cost.cpu().numpy().view(np.uint32) == ref).all())
+        return stats, exact
+
+    for sol in range(6):
+        stats, exact = run_solution(sol)
+        ms = statistics.median(s.kernel_ms for s, _ in stats)
+        st, info = stats[-1]
+        rows[nps.SOLUTION_NAMES[sol]] = {
+            "solution": sol, "ms": ms, "gteps": m_r / ms / 1e6, "exact": exact, "iterations": st.iterations,
+            "edges_scanned_per_m_r": st.edges_scanned / max(m_r, 1), "deferred_rows": info.deferred,
+            "child_launches": info.child_launches, "launch_fallbacks": info.launch_fallbacks,
+            "host_reads": info.host_reads}
+    wpath = os.path.join(ROOT, "nested-parallelism_b200", "policy_weights.npz")
+    arms = [("plain", nps.Params(device=local, **DEFAULT_PARAMS["rmat"]))]
+    if os.path.exists(wpath):
+        pol.load_into_kernel(pol.MLPWeights.load(wpath), local)
+        arms.append(("learned", nps.Params(device=local, policy=nps.POLICY_LEARNED, light_heavy=False,
+                                           **DEFAULT_PARAMS["rmat"])))
+    for name, p in arms:
+        ms_l = []
+        for i in range(3 + reps):
+            st = nps.sssp_device(dg.row_ptr, dg.col, dg.w, g.n, g.m, g.source, dg.dist, p)
+            if i >= 3:
+                ms_l.append(st.kernel_ms)
+        exact = bool((dg.dist.cpu().numpy().view(np.uint32) == ref).all())
+        ms = statistics.median(ms_l)
+        rows[f"sssp_np_consolidate_gpu ({name})"] = {
+            "solution": 6, "ms": ms, "gteps": m_r / ms / 1e6, "exact": exact, "iterations": st.iterations,
+            "edges_scanned_per_m_r": st.edges_scanned / max(m_r, 1)}
+    head = rows[f"sssp_np_consolidate_gpu ({arms[-1][0]})"]
+    if rank == 0:
+        print(json.dumps({"metric": "SSSP GTEPS per SSSP_GPU solution (ablation)", "value": head["gteps"],
+                          "unit": "GTEPS", "n_gpus": ws, "steps": reps, "warmup": 1, "ms_per_step": head["ms"],
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+                          "data": "synthetic", "config": cfg, "ablation": rows,
+                          "all_exact": all(r["exact"] for r in rows.values())}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -509,6 +591,8 @@ def main():
         return bench_batch(a, nps, ws, rank, local, desc)
     if kind == "degree":
         return bench_degree(a, nps, ws, rank, local, desc)
+    if kind == "solutions":
+        return bench_solutions(a, nps, ws, rank, local, desc)
     prm = dict(DEFAULT_PARAMS[kind])
     if a.delta is not None:
         prm["delta"] = a.delta

@@ -229,6 +229,51 @@ nps_status nps_sssp_noalloc(const int32_t* d_row_ptr, const int32_t* d_col, cons
                             int32_t n, int64_t m, int32_t src, uint32_t* d_dist, const nps_params* p,
                             nps_stats* st);
 
+/* ---- the dispatcher's other solutions -------------------------------------
+ * SSSP_GPU()'s `solution` switch (apps/sssp/src/gpu/sssp_wrapper.cu:548-583):
+ * 0-5 are the reference's earlier load-balancing schemes (sssp_wrapper.cu:151-473,
+ * kernels sssp_kernel.cu:34-327 and :626-658), kept for ablation against 6.  All
+ * iterate the same unordered frontier (a queue rebuilt from per-vertex update
+ * flags every iteration) and differ in how a queued row is mapped to threads;
+ * rows of at least p->threshold edges are the "large" ones. */
+enum {
+  NPS_SOLUTION_TQUEUE = 0,          /* one thread walks each queued row (sssp_tqueue_gpu) */
+  NPS_SOLUTION_DUAL_QUEUE = 1,      /* small rows by a thread, large rows by a 64-thread CTA each,
+                                       from two queues (sssp_dual_queue_gpu) */
+  NPS_SOLUTION_SHARED_DELAYED = 2,  /* large rows deferred to the CTA's shared buffer, then walked
+                                       by the whole CTA (sssp_shared_delayed_buffer_gpu) */
+  NPS_SOLUTION_GLOBAL_DELAYED = 3,  /* large rows deferred to one device buffer, walked by a second
+                                       kernel, a 64-thread CTA per row (sssp_global_delayed_buffer_gpu) */
+  NPS_SOLUTION_NP_NAIVE = 4,        /* one child grid per large row, device-side launch (sssp_np_naive_gpu) */
+  NPS_SOLUTION_NP_OPT = 5,          /* one child grid per CTA over its large rows (sssp_np_opt_gpu) */
+  NPS_SOLUTION_CONSOLIDATE = 6      /* workload consolidation: nps_sssp / nps_sssp_state */
+};
+
+typedef struct nps_solution_info {
+  uint64_t deferred;          /* rows handed to a large-row path (high queue, buffer or child grid) */
+  uint64_t child_launches;    /* device-side launches that started (solutions 4 and 5) */
+  uint64_t launch_fallbacks;  /* device-side launches the runtime refused (pending-launch limit);
+                                 the launching thread walked those rows itself */
+  uint32_t host_reads;        /* times the host read the frontier size back */
+  uint32_t pad;
+} nps_solution_info;
+
+/* Solution `solution` (0-6) from a source; arguments as nps_sssp.  p->threshold,
+ * p->block_size (threads of the row-per-thread CTAs, a multiple of 32 in
+ * [64, 1024]), device, stream, device_ptrs and timeout_s (wall-clock bound of
+ * the whole call) apply to 0-5; 6 forwards to nps_sssp with all of p.  info may
+ * be NULL. */
+nps_status nps_sssp_solution(int32_t solution, const int32_t* row_ptr, const int32_t* col,
+                             const uint32_t* w, int32_t n, int64_t m, int32_t src,
+                             const nps_params* p, uint32_t* dist_out, nps_stats* st,
+                             nps_solution_info* info);
+
+/* The same from an existing state, as nps_sssp_state (device pointers only). */
+nps_status nps_sssp_solution_state(int32_t solution, const int32_t* d_row_ptr, const int32_t* d_col,
+                                   const uint32_t* d_w, int32_t n, int64_t m, uint32_t* d_cost,
+                                   uint8_t* d_update, const nps_params* p, nps_stats* st,
+                                   nps_solution_info* info);
+
 /* ---- batched SSSP -------------------------------------------------------- */
 typedef struct nps_instance {
   const int32_t* row_ptr;  /* device pointers */

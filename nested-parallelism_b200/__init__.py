@@ -24,20 +24,29 @@ from typing import Iterable, List, Optional, Sequence
 import numpy as np
 
 from ._native import (NPS_INF, NPS_MLP_HID, NPS_MLP_IN, NPS_MLP_OUT, NpsError, check, lib,
-                      nps_degree_info, nps_graph, nps_instance, nps_params, nps_stats, nps_trace_rec)
+                      nps_degree_info, nps_graph, nps_instance, nps_params, nps_solution_info, nps_stats,
+                      nps_trace_rec)
 
 INF = NPS_INF
 THRESHOLD = 64
 CONSOLIDATE_WARP, CONSOLIDATE_BLOCK, CONSOLIDATE_GRID, CONSOLIDATE_HYBRID = 0, 1, 2, 3
 POLICY_PLAIN, POLICY_LEARNED = 0, 1
-SOLUTION_CONSOLIDATE = 6  # `-s 6`, apps/sssp/src/gpu/sssp.cpp:38
+# `-s <solution>` of the reference CLI (apps/sssp/src/gpu/sssp.cpp:38), the cases of
+# SSSP_GPU()'s switch (apps/sssp/src/gpu/sssp_wrapper.cu:554-566)
+(SOLUTION_TQUEUE, SOLUTION_DUAL_QUEUE, SOLUTION_SHARED_DELAYED, SOLUTION_GLOBAL_DELAYED,
+ SOLUTION_NP_NAIVE, SOLUTION_NP_OPT, SOLUTION_CONSOLIDATE) = range(7)
+SOLUTION_NAMES = ("sssp_tqueue_gpu", "sssp_dual_queue_gpu", "sssp_shared_delayed_buffer_gpu",
+                  "sssp_global_delayed_buffer_gpu", "sssp_np_naive_gpu", "sssp_np_opt_gpu",
+                  "sssp_np_consolidate_gpu")
 
 __all__ = [
     "INF", "THRESHOLD", "CONSOLIDATE_WARP", "CONSOLIDATE_BLOCK", "CONSOLIDATE_GRID",
     "CONSOLIDATE_HYBRID", "POLICY_PLAIN", "POLICY_LEARNED", "Graph", "Params", "Stats",
     "NpsError", "gen_uniform", "gen_rmat", "gen_grid", "convertCSR", "readInputDIMACS9",
     "readInputDIMACS10", "readInputSLNDC", "writeDIMACS9", "sssp", "sssp_device", "SSSP_GPU",
-    "sssp_np_consolidate_gpu", "sssp_batch", "trace_read", "fnv1a", "delta_schedule", "degree_stats", "abi_version", "lib",
+    "sssp_np_consolidate_gpu", "sssp_solution", "sssp_solution_state", "SolutionInfo",
+    "SOLUTION_TQUEUE", "SOLUTION_DUAL_QUEUE", "SOLUTION_SHARED_DELAYED", "SOLUTION_GLOBAL_DELAYED",
+    "SOLUTION_NP_NAIVE", "SOLUTION_NP_OPT", "SOLUTION_CONSOLIDATE", "SOLUTION_NAMES", "sssp_batch", "trace_read", "fnv1a", "delta_schedule", "degree_stats", "abi_version", "lib",
 ]
 
 
@@ -295,13 +304,66 @@ def sssp_device(row_ptr, col, w, n: int, m: int, src: int, dist_out,
     return Stats.from_c(st)
 
 
+@dataclass
+class SolutionInfo:
+    """How solutions 0-5 handled large rows (nps_solution_info)."""
+    deferred: int = 0
+    child_launches: int = 0
+    launch_fallbacks: int = 0
+    host_reads: int = 0
+
+    @staticmethod
+    def from_c(s: nps_solution_info) -> "SolutionInfo":
+        return SolutionInfo(int(s.deferred), int(s.child_launches), int(s.launch_fallbacks), int(s.host_reads))
+
+
+def sssp_solution(g: Graph, solution: int, src: Optional[int] = None,
+                  params: Optional[Params] = None) -> tuple:
+    """One run of SSSP_GPU()'s solution `solution` (0-6, sssp_wrapper.cu:548-583)
+    on host arrays: (uint32 distances, Stats, SolutionInfo).  Solutions 0-5 use
+    params.threshold (the large-row degree, THRESHOLD = 64 in the reference) and
+    params.block_size (threads of the row-per-thread CTAs); 6 is sssp()."""
+    p = params or Params()
+    src = g.source if src is None else src
+    n = g.noNodeTotal
+    row = np.ascontiguousarray(g.vertexArray, dtype=np.int32)
+    col = np.ascontiguousarray(g.edgeArray, dtype=np.int32)
+    w = np.ascontiguousarray(g.weightArray, dtype=np.uint32)
+    dist = np.empty(n, dtype=np.uint32)
+    st, info = nps_stats(), nps_solution_info()
+    cp = p.to_c(device_ptrs=False)
+    check(lib.nps_sssp_solution(solution, row.ctypes.data, col.ctypes.data, w.ctypes.data, n, col.shape[0], src,
+                                C.byref(cp), dist.ctypes.data, C.byref(st), C.byref(info)),
+          f"sssp_solution({solution})")
+    return dist, Stats.from_c(st), SolutionInfo.from_c(info)
+
+
+def sssp_solution_state(solution: int, d_vertexArray, d_edgeArray, d_weightArray, d_costArray, d_update,
+                        noNodeTotal: int, noEdgeTotal: int, params: Optional[Params] = None,
+                        stream: Optional[int] = None) -> tuple:
+    """The state form of solution `solution` (device arrays as prepare_gpu()
+    leaves them, as sssp_np_consolidate_gpu): costs updated in place, d_update
+    cleared.  Returns (Stats, SolutionInfo)."""
+    p = params or Params()
+    st, info = nps_stats(), nps_solution_info()
+    cp = p.to_c(device_ptrs=True, stream=stream)
+    check(lib.nps_sssp_solution_state(solution, _ptr(d_vertexArray), _ptr(d_edgeArray), _ptr(d_weightArray),
+                                      noNodeTotal, noEdgeTotal, _ptr(d_costArray), _ptr(d_update), C.byref(cp),
+                                      C.byref(st), C.byref(info)), f"sssp_solution_state({solution})")
+    return Stats.from_c(st), SolutionInfo.from_c(info)
+
+
 def SSSP_GPU(g: Graph, solution: int = SOLUTION_CONSOLIDATE, level: int = CONSOLIDATE_BLOCK,
              params: Optional[Params] = None) -> np.ndarray:
     """graph.costArray after one SSSP_GPU() run (sssp_wrapper.cu:548-583): int32
-    costs with INF = 2^30 for unreachable vertices.  Only solution 6 (workload
-    consolidation) is provided by this library."""
+    costs with INF = 2^30 for unreachable vertices.  `solution` selects the case
+    of the reference's switch: 0-5 the earlier load-balancing schemes
+    (sssp_solution), 6 workload consolidation at `level`."""
+    if solution < 0 or solution > SOLUTION_CONSOLIDATE:
+        raise NpsError(1, f"SSSP_GPU: solution must be 0..6, got {solution}")
     if solution != SOLUTION_CONSOLIDATE:
-        raise NpsError(1, f"SSSP_GPU: solution {solution} is not provided (only 6, workload consolidation)")
+        dist, _, _ = sssp_solution(g, solution, g.source, params)
+        return dist.view(np.int32)
     p = params or Params(level=level)
     dist, _ = sssp(g, g.source, p)
     return dist.view(np.int32)

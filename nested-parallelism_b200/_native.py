@@ -82,6 +82,13 @@ class nps_degree_info(C.Structure):
     ]
 
 
+class nps_solution_info(C.Structure):
+    _fields_ = [
+        ("deferred", C.c_uint64), ("child_launches", C.c_uint64), ("launch_fallbacks", C.c_uint64),
+        ("host_reads", C.c_uint32), ("pad", C.c_uint32),
+    ]
+
+
 _P = C.c_void_p
 _I32, _I64, _U32, _U64, _F, _D = C.c_int32, C.c_int64, C.c_uint32, C.c_uint64, C.c_float, C.c_double
 
@@ -106,6 +113,10 @@ SIGNATURES = {
                             C.POINTER(nps_stats)]),
     "nps_sssp_state": (_I32, [_P, _P, _P, _I32, _I64, _P, _P, C.POINTER(nps_params),
                               C.POINTER(nps_stats)]),
+    "nps_sssp_solution": (_I32, [_I32, _P, _P, _P, _I32, _I64, _I32, C.POINTER(nps_params), _P,
+                                 C.POINTER(nps_stats), C.POINTER(nps_solution_info)]),
+    "nps_sssp_solution_state": (_I32, [_I32, _P, _P, _P, _I32, _I64, _P, _P, C.POINTER(nps_params),
+                                       C.POINTER(nps_stats), C.POINTER(nps_solution_info)]),
     "nps_trace_read": (_I32, [_I32, C.POINTER(nps_trace_rec), _I32, C.POINTER(_I32)]),
     "nps_sssp_noalloc": (_I32, [_P, _P, _P, _I32, _I64, _I32, _P, C.POINTER(nps_params), C.POINTER(nps_stats)]),
     "nps_sssp_batch": (_I32, [C.POINTER(nps_instance), _I32, C.POINTER(nps_params), _I32,

@@ -67,3 +67,20 @@ def test_compute_calls_without_a_gpu_return_a_status(nps):
         nps.sssp(g, 0)
     assert ei.value.status == 5  # NPS_ERR_NO_DEVICE: reported, not a crash or exit
     assert "CUDA" in str(ei.value) or "device" in str(ei.value)
+
+
+def test_solution_arguments_are_checked_before_the_device(nps):
+    """nps_sssp_solution rejects bad solutions and parameters with status 1
+    before it touches a device."""
+    g = nps.gen_uniform(100, 500, 10, 1)
+    cases = ((7, {}), (-1, {}), (0, {"block_size": 100}), (1, {"block_size": 32}), (2, {"block_size": 2048}),
+             (3, {"threshold": 0}), (4, {"timeout_s": 0.0}))
+    for sol, kw in cases:
+        with pytest.raises(nps.NpsError) as ei:
+            nps.sssp_solution(g, sol, 0, nps.Params(**kw))
+        assert ei.value.status == 1, (sol, kw)
+    with pytest.raises(nps.NpsError) as ei:
+        nps.sssp_solution(g, 0, g.n)  # source out of range
+    assert ei.value.status == 1
+    with pytest.raises(nps.NpsError):
+        nps.SSSP_GPU(g, solution=9)

@@ -16,7 +16,8 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 def _build(out, level):
     cmd = ["g++", "-O2", "-std=c++17", f"-DCONSOLIDATE_LEVEL={level}", "-I", os.path.join(ROOT, "include"),
            "-I", os.path.join(CUDA, "include"), os.path.join(ROOT, "tests", "compat", "harness.cpp"),
-           os.path.join(PKG, "compat", "sssp_np_consolidate_gpu.cpp"), "-o", str(out), "-L", PKG, "-lnps",
+           os.path.join(PKG, "compat", "sssp_np_consolidate_gpu.cpp"),
+           os.path.join(PKG, "compat", "sssp_solutions_gpu.cpp"), "-o", str(out), "-L", PKG, "-lnps",
            "-L", os.path.join(CUDA, "lib64"), "-lcudart", f"-Wl,-rpath,{PKG}:{os.path.join(CUDA, 'lib64')}"]
     subprocess.run(cmd, check=True, capture_output=True, text=True)
     return str(out)
@@ -43,5 +44,20 @@ def test_shim_matches_the_oracle(nps, oracle, cuda_device, harnesses, level, kin
     g = nps.gen_rmat(size, 16, seed=seed) if kind == "rmat" else nps.gen_uniform(size, 8 * size, 100, seed)
     ref = oracle.sssp_heap(g.row_ptr, g.col, g.w, g.source)
     assert int(f["status"]) == 0 and int(f["source"]) == g.source
+    assert int(f["fnv1a"], 16) == nps.fnv1a(ref)
+    assert int(f["update_left"]) == 0 and int(f["iterations"]) > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("solution", [0, 1, 2, 3, 4, 5])
+def test_solution_shims_match_the_oracle(nps, oracle, cuda_device, harnesses, solution):
+    """SSSP_GPU()'s cases 0-5 (sssp_wrapper.cu:554-564) through the drop-in shims."""
+    r = subprocess.run([harnesses[1], "rmat", "14", "5", str(solution)], capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 0, r.stderr
+    f = dict(zip(r.stdout.split()[0::2], r.stdout.split()[1::2]))
+    g = nps.gen_rmat(14, 16, seed=5)
+    ref = oracle.sssp_heap(g.row_ptr, g.col, g.w, g.source)
+    assert int(f["status"]) == 0
     assert int(f["fnv1a"], 16) == nps.fnv1a(ref)
     assert int(f["update_left"]) == 0 and int(f["iterations"]) > 0
