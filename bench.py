@@ -63,6 +63,9 @@ WORKLOADS = {
                     "ablation: SSSP_GPU solutions 0-6 (thread queue, dual queue, shared / global delayed "
                     "buffer, naive / per-block nested launch, consolidation plain and learned) on R-MAT scale 22, "
                     "edge factor 16, seed 1000"),
+    "bfs22": ("bfs", dict(scale=22, edge_factor=16, seed=1000),
+              "breadth-first levels (bfs-rec's bfs_rec_dp_cons_gpu) on R-MAT scale 22, edge factor 16, "
+              "seed 1000, source 0; unit edge weights, no weight array read"),
     "batch64": ("batch", dict(count=64, seed=7),
                 "64 R-MAT instances (a=.57 b=.19 c=.19), scale U{12..18}, edge factor {4,8,16,32}, "
                 "w in [1,255], random sources, seed 7; one persistent CUDA-graph launch per shard"),
@@ -568,6 +571,119 @@ def bench_solutions(a, nps, ws, rank, local, desc):
     return 0
 
 
+def bench_bfs(a, nps, ws, rank, local, desc):
+    """Breadth-first levels on the SSSP engine (nps_bfs): the unordered frontier
+    (the default, headline arm) and one-level buckets, both checked against the oracle.
+    value = reached out-edges per second of device time; B_alg = 8 m_r + 12 n_r +
+    4 n (column index and level per reached edge; row offsets, level read and
+    write per reached vertex; the level array once)."""
+    _, args, _ = WORKLOADS[a.workload]
+    g = nps.gen_rmat(args["scale"], args["edge_factor"], seed=args["seed"])
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    want = oracle.bfs_levels(g.row_ptr, g.col, g.source)
+    reached = want != oracle.BFS_UNDEFINED
+    n_r, m_r = int(reached.sum()), int(np.diff(g.row_ptr)[reached].sum())
+    cfg = {"workload": a.workload, "description": desc, "n": g.n, "m": g.m, "m_reached": m_r, "n_reached": n_r,
+           "source": g.source}
+    if a.impl == "reference":
+        if rank == 0:
+            use_ref = oracle.have_reference_bfs()
+            fn = (lambda: oracle.ref_bfs_cpu(g.row_ptr, g.col, g.source)[1]) if use_ref else \
+                (lambda: oracle.timed(oracle.bfs_levels, g.row_ptr, g.col, g.source)[1])
+            for _ in range(min(a.warmup, 1)):
+                fn()
+            secs = [fn() for _ in range(a.steps)]
+            value = m_r * a.steps / sum(secs) / 1e9
+            kind = "reference" if use_ref else "port"
+            cpu = {"value": value, "unit": "GTEPS", "cores": 1, "kind": kind,
+                   "sample": ("the reference's bfs_cpu (apps/bfs-rec/src/gpu/bfs_rec.cpp:100-119, built from its "
+                              "sources), one full BFS per step, 1 thread") if use_ref else
+                             "the oracle's numpy level-synchronous BFS, one full BFS per step"}
+            print(json.dumps({"impl": "reference", "metric": "BFS GTEPS", "value": value, "unit": "GTEPS",
+                              "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+                              "ms_per_step": 1e3 * sum(secs) / a.steps, "higher_is_better": True,
+                              "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+                              "config": dict(cfg, parallelism="host cores"), "cpu_baseline": cpu,
+                              "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}))
+        return 0
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    row = torch.from_numpy(g.row_ptr.view(np.int32)).to(dev)
+    col = torch.from_numpy(g.col.view(np.int32)).to(dev)
+    level = torch.empty(g.n, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    arms = {"unordered": nps.bfs_params(device=local),
+            "levels": nps.bfs_params(device=local, delta=1)}
+
+    def timed(p, clk=None):
+        with torch.cuda.stream(stream):
+            for _ in range(a.warmup):
+                nps.bfs_device(row, col, g.n, g.m, g.source, level, p, stream=stream.cuda_stream)
+        torch.cuda.synchronize(dev)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+        st = None
+        with (clk if clk is not None else contextlib.nullcontext()):
+            with torch.cuda.stream(stream):
+                for i in range(a.steps):
+                    flush.fill_(i & 0x7F)
+                    evs[i][0].record(stream)
+                    st = nps.bfs_device(row, col, g.n, g.m, g.source, level, p, stream=stream.cuda_stream)
+                    evs[i][1].record(stream)
+            torch.cuda.synchronize(dev)
+        exact = bool((level.cpu().numpy() == want).all())
+        return [s_.elapsed_time(e_) for s_, e_ in evs], st, exact
+
+    lv_ms, lv_st, lv_exact = timed(arms["levels"])
+    clk = ClockSampler(local)
+    ms, st, exact = timed(arms["unordered"], clk)
+    per = sum(ms) / a.steps
+    value = ws * m_r / (per * 1e-3) / 1e9
+
+    def pinned(x):
+        return torch.from_numpy(np.ascontiguousarray(x).view(np.int32)).pin_memory().numpy()
+    hg = nps.Graph(pinned(g.row_ptr), pinned(g.col), np.zeros(0, np.uint32), g.source)
+    nps.bfs(hg, g.source, arms["unordered"])
+    t0 = time.perf_counter()
+    e2e_steps = a.e2e_steps or a.steps
+    for _ in range(e2e_steps):
+        lv, _ = nps.bfs(hg, g.source, arms["unordered"])
+    e2e_ms = (time.perf_counter() - t0) / e2e_steps * 1e3
+    e2e_ok = bool((lv == want).all())
+    peak, peak_src = load_peaks()
+    b_alg = 8 * m_r + 12 * n_r + 4 * g.n
+    achieved = b_alg / (per * 1e-3) / 1e9
+    cpu = None
+    if rank == 0 and not a.no_cpu_baseline and oracle.have_reference_bfs():
+        lref, tcpu = oracle.ref_bfs_cpu(g.row_ptr, g.col, g.source)
+        cpu = {"value": m_r / tcpu / 1e9, "unit": "GTEPS", "cores": 1, "kind": "reference", "seconds": tcpu,
+               "sample": "one full BFS by the reference's bfs_cpu (bfs_rec.cpp:100-119), 1 thread",
+               "exact_vs_gpu": bool((lref == want).all())}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "BFS GTEPS", "value": value, "unit": "GTEPS", "n_gpus": ws, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": per, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": dict(cfg, params=dataclasses.asdict(arms["unordered"]), iterations=st.iterations,
+                           edges_scanned=st.edges_scanned, exact_vs_oracle=exact,
+                           l2="flushed between steps (256 MB write)"),
+            "one_level_buckets": {"value": ws * m_r / (sum(lv_ms) / a.steps * 1e-3) / 1e9, "unit": "GTEPS",
+                                  "ms_per_step": sum(lv_ms) / a.steps, "edges_scanned": lv_st.edges_scanned,
+                                  "iterations": lv_st.iterations, "buckets": lv_st.buckets,
+                                  "exact_vs_oracle": lv_exact},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_source": peak_src, "b_alg_bytes": b_alg,
+                         "b_alg_formula": "8*m_r + 12*n_r + 4*n"},
+            "e2e": {"value": ws * m_r / (e2e_ms * 1e-3) / 1e9, "unit": "GTEPS", "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": 4 * (g.n + 1) + 4 * g.m, "d2h_bytes_per_step": 4 * g.n,
+                    "exact_vs_oracle": e2e_ok, "call": "nps.bfs(host Graph, pinned)"},
+            "gpu_launches": 2 * a.steps, "clocks": clk.summary(), "cpu_baseline": cpu}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -593,6 +709,8 @@ def main():
         return bench_degree(a, nps, ws, rank, local, desc)
     if kind == "solutions":
         return bench_solutions(a, nps, ws, rank, local, desc)
+    if kind == "bfs":
+        return bench_bfs(a, nps, ws, rank, local, desc)
     prm = dict(DEFAULT_PARAMS[kind])
     if a.delta is not None:
         prm["delta"] = a.delta

@@ -23,6 +23,13 @@
  *   nps_read_dimacs9 / _dimacs10 / _slndc
  *                             replace readInputDIMACS9/10/SLNDC() + convertCSR()
  *                                       common/global.cpp:29-64, :66-105, :107-190, :192-235
+ *   nps_sssp_solution(_state) replace cases 0-5 of SSSP_GPU()'s switch (sssp_tqueue_gpu ...
+ *                             sssp_np_opt_gpu)      apps/sssp/src/gpu/sssp_wrapper.cu:151-473
+ *   nps_bfs                   replaces void bfs_rec_dp_cons_gpu(void), the bfs-rec
+ *                             application's consolidated BFS on the same engine
+ *                                       apps/bfs-rec/src/gpu/bfs_rec_wrapper.cu:170-229
+ *   nps_degree_stats          replaces the graph analyzer's getStatInfo()
+ *                                       utility/graph-analyzer/analyzer.cpp:75-138
  *   nps_graph                 replaces struct _GRAPH_'s CSR members and the
  *                             noNodeTotal / noEdgeTotal / source globals
  *                                       common/global.h:28-58
@@ -228,6 +235,18 @@ nps_status nps_trace_read(int32_t device, nps_trace_rec* out, int32_t cap, int32
 nps_status nps_sssp_noalloc(const int32_t* d_row_ptr, const int32_t* d_col, const uint32_t* d_w,
                             int32_t n, int64_t m, int32_t src, uint32_t* d_dist, const nps_params* p,
                             nps_stats* st);
+
+/* ---- breadth-first levels ---------------------------------------------------
+ * The bfs-rec application's consolidated BFS (bfs_rec_dp_cons_gpu,
+ * apps/bfs-rec/src/gpu/bfs_rec_wrapper.cu:170-229) on the same persistent engine:
+ * every edge weighs 1 and no weight array is read.  level_out[n] receives the hop
+ * count from src, NPS_BFS_UNDEFINED for unreachable vertices (bfs_rec.h:13); the
+ * result equals the reference's bfs_cpu (apps/bfs-rec/src/gpu/bfs_rec.cpp:100-119).
+ * Arguments as nps_sssp.  With unit weights the unordered frontier (delta 0)
+ * already advances one level per iteration; delta = 1 gives one bucket per level. */
+#define NPS_BFS_UNDEFINED 0x7FFFFFFF
+nps_status nps_bfs(const int32_t* row_ptr, const int32_t* col, int32_t n, int64_t m, int32_t src,
+                   const nps_params* p, int32_t* level_out, nps_stats* st);
 
 /* ---- the dispatcher's other solutions -------------------------------------
  * SSSP_GPU()'s `solution` switch (apps/sssp/src/gpu/sssp_wrapper.cu:548-583):

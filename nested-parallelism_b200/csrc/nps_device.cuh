@@ -90,7 +90,7 @@ struct __align__(128) Counters {
 struct InstDesc {
   const int32_t* row_ptr;
   const int32_t* col;
-  const uint32_t* w;
+  const uint32_t* w;     // null: every edge weighs 1 (breadth-first levels)
   uint32_t* dist;
   uint8_t* update;      // state mode: initial frontier flags, cleared in place
   int32_t n;
@@ -509,7 +509,8 @@ __device__ __forceinline__ void relax_and_push(const InstDesc& I, const IterCtx&
 
 // Load the 16-byte chunk at edge index c (4-aligned) of the column and weight
 // arrays: one int4 load each when aligned and in bounds, else element-wise
-// loads of the positions inside [s, e).
+// loads of the positions inside [s, e).  A null weight array means every edge
+// weighs 1 (breadth-first levels), and no weight is read.
 __device__ __forceinline__ void load_chunk(const InstDesc& I, bool act, int32_t c, int32_t s, int32_t e,
                                            int4& cv, int4& wv) {
   cv = make_int4(0, 0, 0, 0);
@@ -517,13 +518,13 @@ __device__ __forceinline__ void load_chunk(const InstDesc& I, bool act, int32_t 
   if (!act) return;
   if (I.vec_ok && c + 4 <= I.m) {
     cv = ld_stream_v4(I.col + c);
-    wv = ld_stream_v4((const int32_t*)I.w + c);
+    wv = I.w ? ld_stream_v4((const int32_t*)I.w + c) : make_int4(1, 1, 1, 1);
   } else {
     const int32_t* wp = (const int32_t*)I.w;
-    if (c >= s && c < e) { cv.x = ld_stream(I.col + c); wv.x = ld_stream(wp + c); }
-    if (c + 1 >= s && c + 1 < e) { cv.y = ld_stream(I.col + c + 1); wv.y = ld_stream(wp + c + 1); }
-    if (c + 2 >= s && c + 2 < e) { cv.z = ld_stream(I.col + c + 2); wv.z = ld_stream(wp + c + 2); }
-    if (c + 3 >= s && c + 3 < e) { cv.w = ld_stream(I.col + c + 3); wv.w = ld_stream(wp + c + 3); }
+    if (c >= s && c < e) { cv.x = ld_stream(I.col + c); wv.x = wp ? ld_stream(wp + c) : 1; }
+    if (c + 1 >= s && c + 1 < e) { cv.y = ld_stream(I.col + c + 1); wv.y = wp ? ld_stream(wp + c + 1) : 1; }
+    if (c + 2 >= s && c + 2 < e) { cv.z = ld_stream(I.col + c + 2); wv.z = wp ? ld_stream(wp + c + 2) : 1; }
+    if (c + 3 >= s && c + 3 < e) { cv.w = ld_stream(I.col + c + 3); wv.w = wp ? ld_stream(wp + c + 3) : 1; }
   }
 }
 
@@ -823,7 +824,7 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         nb[j] = valid[j] ? ld_stream(I.col + ei[j]) : 0;
-        nd[j] = valid[j] ? (uint32_t)ld_stream((const int32_t*)I.w + ei[j]) : 0u;
+        nd[j] = valid[j] ? (I.w ? (uint32_t)ld_stream((const int32_t*)I.w + ei[j]) : 1u) : 0u;
       }
 #pragma unroll
       for (int j = 0; j < 4; ++j) {

@@ -558,9 +558,19 @@ extern "C" nps_status nps_ctx_destroy(nps_ctx* ctx) {
   return NPS_OK;
 }
 
-extern "C" nps_status nps_sssp_ctx(nps_ctx* c, const int32_t* row_ptr, const int32_t* col,
-                                   const uint32_t* w, int32_t n, int64_t m, int32_t src,
-                                   const nps_params* pin, uint32_t* dist_out, nps_stats* st) {
+namespace {
+
+// Breadth-first levels from unit-weight distances: unreachable vertices (NPS_INF)
+// get the reference's UNDEFINED (apps/bfs-rec/src/gpu/bfs_rec.h:13).
+__global__ void bfs_levels_kernel(uint32_t* d, int32_t n) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+    if (d[v] >= NPS_INF) d[v] = (uint32_t)NPS_BFS_UNDEFINED;
+}
+
+// nps_sssp_ctx, and with bfs = true nps_bfs (w unused: every edge weighs 1).
+nps_status sssp_ctx_impl(nps_ctx* c, const int32_t* row_ptr, const int32_t* col, const uint32_t* w, int32_t n,
+                         int64_t m, int32_t src, const nps_params* pin, uint32_t* dist_out, nps_stats* st,
+                         bool bfs) {
   nps_clear_error();
   nps_params p;
   if (pin) p = *pin;
@@ -571,7 +581,8 @@ extern "C" nps_status nps_sssp_ctx(nps_ctx* c, const int32_t* row_ptr, const int
   if (n <= 0) return nps_fail(NPS_ERR_INVALID_ARG, "n must be positive");
   if (m < 0 || m >= (int64_t)INT32_MAX) return nps_fail(NPS_ERR_INVALID_ARG, "m must be in [0, 2^31-1)");
   if (src < 0 || src >= n) return nps_fail(NPS_ERR_INVALID_ARG, "source vertex out of range");
-  if (!row_ptr || !dist_out || (m > 0 && (!col || !w))) return nps_fail(NPS_ERR_INVALID_ARG, "null array");
+  if (bfs) w = nullptr;
+  if (!row_ptr || !dist_out || (m > 0 && (!col || (!w && !bfs)))) return nps_fail(NPS_ERR_INVALID_ARG, "null array");
   std::lock_guard<std::mutex> lk(c->mu);
   NPS_CUDA(cudaSetDevice(c->device));
   cudaStream_t s = p.stream ? (cudaStream_t)p.stream : c->stream;
@@ -586,19 +597,24 @@ extern "C" nps_status nps_sssp_ctx(nps_ctx* c, const int32_t* row_ptr, const int
     if (row_ptr[0] != 0 || row_ptr[n] != (int32_t)m)
       return nps_fail(NPS_ERR_FORMAT, "malformed CSR: row_ptr[0] must be 0 and row_ptr[n] must be m");
     if ((e = c->g_row.ensure((size_t)n + 1, false, s)) || (e = c->g_col.ensure((size_t)m, false, s)) ||
-        (e = c->g_w.ensure((size_t)m, false, s)) || (e = c->g_dist.ensure((size_t)n, false, s)))
+        (!bfs && (e = c->g_w.ensure((size_t)m, false, s))) || (e = c->g_dist.ensure((size_t)n, false, s)))
       return e;
     NPS_CUDA(cudaMemcpyAsync(c->g_row.p, row_ptr, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, s));
     if (m > 0) {
       NPS_CUDA(cudaMemcpyAsync(c->g_col.p, col, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
-      NPS_CUDA(cudaMemcpyAsync(c->g_w.p, w, sizeof(uint32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
+      if (!bfs) NPS_CUDA(cudaMemcpyAsync(c->g_w.p, w, sizeof(uint32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
     }
     drow = c->g_row.p;
     dcol = c->g_col.p;
-    dw = c->g_w.p;
+    dw = bfs ? nullptr : c->g_w.p;
     ddist = c->g_dist.p;
   }
   if ((e = run_single(c, s, drow, dcol, dw, n, m, src, ddist, nullptr, 0, p, st, true))) return e;
+  if (bfs) {
+    const int lg = (int)std::min<int64_t>(((int64_t)n + 255) / 256, (int64_t)c->di.sms * 8);
+    bfs_levels_kernel<<<lg, 256, 0, s>>>(ddist, n);
+    NPS_CUDA(cudaGetLastError());
+  }
   if (!p.device_ptrs)
     NPS_CUDA(cudaMemcpyAsync(dist_out, ddist, sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToHost, s));
   NPS_CUDA(cudaEventRecord(c->ev[3], s));
@@ -613,6 +629,27 @@ extern "C" nps_status nps_sssp_ctx(nps_ctx* c, const int32_t* row_ptr, const int
   }
   if (k.status) reset_stamps(c, s);
   return status_from_device(k.status);
+}
+
+}  // namespace
+
+extern "C" nps_status nps_sssp_ctx(nps_ctx* c, const int32_t* row_ptr, const int32_t* col,
+                                   const uint32_t* w, int32_t n, int64_t m, int32_t src,
+                                   const nps_params* pin, uint32_t* dist_out, nps_stats* st) {
+  return sssp_ctx_impl(c, row_ptr, col, w, n, m, src, pin, dist_out, st, false);
+}
+
+extern "C" nps_status nps_bfs(const int32_t* row_ptr, const int32_t* col, int32_t n, int64_t m, int32_t src,
+                              const nps_params* p, int32_t* level_out, nps_stats* st) {
+  nps_clear_error();
+  // arguments first, so a bad call is reported as such even without a device
+  nps_status e0 = p ? check_params(*p) : NPS_OK;
+  if (e0) return e0;
+  if (n <= 0 || src < 0 || src >= n) return nps_fail(NPS_ERR_INVALID_ARG, "bfs: n must be positive and src in [0, n)");
+  nps_ctx* c = nullptr;
+  nps_status e = default_ctx(p ? p->device : 0, &c);
+  if (e) return e;
+  return sssp_ctx_impl(c, row_ptr, col, nullptr, n, m, src, p, reinterpret_cast<uint32_t*>(level_out), st, true);
 }
 
 extern "C" nps_status nps_sssp(const int32_t* row_ptr, const int32_t* col, const uint32_t* w, int32_t n,

@@ -9,6 +9,7 @@ in nested-parallelism_b200/ never imports it.
   _ref/libref_sssp.so   the reference's own SSSP_CPU / usssp_cpu / dheap built
                         from its sources by oracle/Makefile (absent if the
                         reference tree was not available when it was built)
+  _ref/libref_bfs.so    the reference's own CPU BFS (bfs-rec's bfs_cpu), likewise
 """
 from __future__ import annotations
 
@@ -21,7 +22,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libref_sssp.so")
+REF_BFS_SO = os.path.join(HERE, "_ref", "libref_bfs.so")
 INF = 0x40000000
+BFS_UNDEFINED = 0x7FFFFFFF  # apps/bfs-rec/src/gpu/bfs_rec.h:13
 
 _P, _I32, _I64, _D = C.c_void_p, C.c_int32, C.c_int64, C.c_double
 
@@ -160,6 +163,61 @@ def ref_dijkstra_dheap(row, col, w, src, d=2):
     t = _load_ref().nps_ref_dijkstra_dheap(n, row.ctypes.data, col.ctypes.data, w.ctypes.data, int(src), int(d),
                                            cost.ctypes.data)
     return cost.view(np.uint32), float(t)
+
+
+def bfs_levels(row, col, src):
+    """Restated bfs_cpu of the bfs-rec application (apps/bfs-rec/src/gpu/bfs_rec.cpp:100-119):
+    the hop count from src, BFS_UNDEFINED for unreachable vertices.  The reference
+    walks a FIFO queue and re-queues a vertex whose level drops; in FIFO order a
+    vertex is first reached at its least hop count, so the levels are those of a
+    level-synchronous sweep, which this restatement runs one frontier at a time
+    in numpy."""
+    row = np.ascontiguousarray(row, dtype=np.int64)
+    col = np.ascontiguousarray(col, dtype=np.int64)
+    n = row.shape[0] - 1
+    level = np.full(n, BFS_UNDEFINED, dtype=np.int32)
+    level[src] = 0
+    frontier = np.array([src], dtype=np.int64)
+    depth = 0
+    while frontier.size:
+        depth += 1
+        starts, ends = row[frontier], row[frontier + 1]
+        lens = ends - starts
+        total = int(lens.sum())
+        if total == 0:
+            break
+        # edge indices of every frontier row, concatenated
+        offs = np.repeat(starts - np.concatenate(([0], np.cumsum(lens)[:-1])), lens)
+        nbr = col[np.arange(total, dtype=np.int64) + offs]
+        nbr = np.unique(nbr[level[nbr] == BFS_UNDEFINED])
+        level[nbr] = depth
+        frontier = nbr
+    return level
+
+
+def have_reference_bfs() -> bool:
+    return os.path.exists(REF_BFS_SO)
+
+
+_ref_bfs = None
+
+
+def ref_bfs_cpu(row, col, src):
+    """The reference's bfs_cpu() on these arrays; returns (levels int32, seconds)."""
+    global _ref_bfs
+    if _ref_bfs is None:
+        if not have_reference_bfs():
+            raise ImportError(f"{REF_BFS_SO} missing: the reference CPU code was not built")
+        lib = C.CDLL(REF_BFS_SO)
+        lib.nps_ref_bfs_cpu.argtypes = [_I32, _I32, _P, _P, _I32, _P]
+        lib.nps_ref_bfs_cpu.restype = _D
+        _ref_bfs = lib
+    row = np.ascontiguousarray(row, dtype=np.int32)
+    col = np.ascontiguousarray(col, dtype=np.int32)
+    n, m = row.shape[0] - 1, col.shape[0]
+    level = np.empty(n, dtype=np.int32)
+    t = _ref_bfs.nps_ref_bfs_cpu(n, m, row.ctypes.data, col.ctypes.data, int(src), level.ctypes.data)
+    return level, float(t)
 
 
 def degree_stats(row):

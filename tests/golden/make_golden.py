@@ -7,7 +7,9 @@ sssp.cpp:13-47 with common/heap.cpp), compiled from its unmodified sources into
 oracle/_ref/libref_sssp.so by oracle/Makefile.  The degree-statistics goldens
 come from the reference's graph analyzer (utility/graph-analyzer/analyzer.cpp),
 built into oracle/_ref/analyzer, run on the reader fixtures and on generated
-graphs written as DIMACS9.  The reader fixtures are small
+graphs written as DIMACS9.  The BFS goldens come from the reference's bfs_cpu
+(apps/bfs-rec/src/gpu/bfs_rec.cpp:100-119), built into oracle/_ref/libref_bfs.so,
+on the same generated graphs and edge cases.  The reader fixtures are small
 synthetic DIMACS9 / DIMACS10 / SNAP files written here; their expected CSR comes
 from the reference's readInputDIMACS9/10/SLNDC() + convertCSR() (common/
 global.cpp:29-235) on the same files.
@@ -132,6 +134,26 @@ def analyzer_goldens():
     return res
 
 
+def bfs_goldens():
+    """Levels from the reference's bfs_cpu on every case graph (FNV-1a of the int32
+    levels viewed as uint32) and on the edge cases (the levels themselves)."""
+    if not oracle.have_reference_bfs():
+        sys.exit("oracle/_ref/libref_bfs.so missing: build it with `make -C oracle` where the reference exists")
+    res = {"cases": {}, "edge_cases": {}}
+    for name, kind, args, src in CASES:
+        g = gen(kind, args)
+        s = g.source if src is None else src
+        lv, _ = oracle.ref_bfs_cpu(g.row_ptr, g.col, s)
+        fin = lv[lv != oracle.BFS_UNDEFINED]
+        res["cases"][name] = {"source": int(s), "levels_fnv1a": oracle.fnv1a(lv.view(np.uint32)),
+                              "n_reached": int(fin.size), "max_level": int(fin.max())}
+    for name, n, s, t, w, src in EDGE_CASES:
+        g = nps.convertCSR(n, s, t, w)
+        lv, _ = oracle.ref_bfs_cpu(g.row_ptr, g.col, src)
+        res["edge_cases"][name] = [int(x) for x in lv]
+    return res
+
+
 def main():
     if not oracle.have_reference():
         sys.exit("oracle/_ref/libref_sssp.so missing: build it with `make -C oracle` where the reference exists")
@@ -162,6 +184,7 @@ def main():
                                  "row_fnv1a": nps.fnv1a(row.view(np.uint32)),
                                  "col_fnv1a": nps.fnv1a(col.view(np.uint32)), "w_fnv1a": nps.fnv1a(w)}
     out["analyzer"] = analyzer_goldens()
+    out["bfs"] = bfs_goldens()
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)
     np.savez_compressed(os.path.join(HERE, "golden_dist.npz"), **dists)

@@ -200,7 +200,8 @@ def test_SSSP_GPU_mirror(nps, oracle, cuda_device, uniform):
     assert cost.dtype == np.int32
     assert (cost.view(np.uint32) == oracle.sssp_heap(uniform.row_ptr, uniform.col, uniform.w, 0)).all()
     with pytest.raises(nps.NpsError):
-        nps.SSSP_GPU(uniform, solution=3)
+        nps.SSSP_GPU(uniform, solution=7)  # the reference's switch has cases 0-6
+    assert (nps.SSSP_GPU(uniform, solution=3) == cost).all()
 
 
 # ---- batch -------------------------------------------------------------------
