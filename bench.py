@@ -66,6 +66,9 @@ WORKLOADS = {
     "bfs22": ("bfs", dict(scale=22, edge_factor=16, seed=1000),
               "breadth-first levels (bfs-rec's bfs_rec_dp_cons_gpu) on R-MAT scale 22, edge factor 16, "
               "seed 1000, source 0; unit edge weights, no weight array read"),
+    "spmv22": ("spmv", dict(scale=22, edge_factor=16, seed=1000),
+               "y = A x in double (the SpMV application's spmv_np_consolidate_gpu) for the R-MAT scale 22, "
+               "edge factor 16, seed 1000 matrix with the reference's data: val[i] = i%13+0.5, x[i] = i%17+0.5"),
     "batch64": ("batch", dict(count=64, seed=7),
                 "64 R-MAT instances (a=.57 b=.19 c=.19), scale U{12..18}, edge factor {4,8,16,32}, "
                 "w in [1,255], random sources, seed 7; one persistent CUDA-graph launch per shard"),
@@ -684,6 +687,110 @@ def bench_bfs(a, nps, ws, rank, local, desc):
     return 0
 
 
+def bench_spmv(a, nps, ws, rank, local, desc):
+    """SpMV on the R-MAT scale-22 matrix at the three consolidation levels (GRID is
+    the headline), device arrays resident, L2 flushed between steps, every y
+    compared bit for bit with the reference's spmv_omp (exact for its data).
+    value = algorithmic bytes / device time, B_alg = 12 m + 20 n + 4: column index
+    and value per nonzero, x read once, y written once, row offsets."""
+    _, args, _ = WORKLOADS[a.workload]
+    g = nps.gen_rmat(args["scale"], args["edge_factor"], seed=args["seed"])
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    val, x = oracle.spmv_data(g.n, g.m)
+    b_alg = 12 * g.m + 20 * g.n + 4
+    cfg = {"workload": a.workload, "description": desc, "n": g.n, "m": g.m, "threshold": 64}
+    if a.impl == "reference":
+        if rank == 0:
+            use_ref = oracle.have_reference_spmv()
+            cores = os.cpu_count() or 1
+            fn = (lambda: oracle.ref_spmv_cpu(g.row_ptr, g.col, cores)[3]) if use_ref else \
+                (lambda: oracle.timed(oracle.spmv, g.row_ptr, g.col, val, x)[1])
+            fn()
+            secs = [fn() for _ in range(a.steps)]
+            value = b_alg * a.steps / sum(secs) / 1e9
+            cpu = {"value": value, "unit": "GB/s", "cores": cores if use_ref else 1,
+                   "kind": "reference" if use_ref else "port",
+                   "sample": "one full y = A x per step by the reference's spmv_omp (apps/SpMV/src/cpu/"
+                             "SpMV_kernel.cpp:26-42, built from its sources) on all host threads" if use_ref else
+                             "one full y = A x per step by the oracle's numpy restatement"}
+            print(json.dumps({"impl": "reference", "metric": "SpMV GB/s", "value": value, "unit": "GB/s",
+                              "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+                              "ms_per_step": 1e3 * sum(secs) / a.steps, "higher_is_better": True,
+                              "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                              "config": dict(cfg, parallelism="host cores"), "cpu_baseline": cpu,
+                              "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}))
+        return 0
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    row = torch.from_numpy(g.row_ptr.view(np.int32)).to(dev)
+    col = torch.from_numpy(g.col.view(np.int32)).to(dev)
+    dv, dx = torch.from_numpy(val).to(dev), torch.from_numpy(x).to(dev)
+    dy = torch.empty(g.n, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    want = oracle.spmv(g.row_ptr, g.col, val, x)
+
+    def timed(p, clk=None):
+        with torch.cuda.stream(stream):
+            for _ in range(a.warmup):
+                nps.spmv_device(row, col, dv, dx, dy, g.n, g.m, p, stream=stream.cuda_stream)
+        torch.cuda.synchronize(dev)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+        with (clk if clk is not None else contextlib.nullcontext()):
+            with torch.cuda.stream(stream):
+                for i in range(a.steps):
+                    flush.fill_(i & 0x7F)
+                    evs[i][0].record(stream)
+                    nps.spmv_device(row, col, dv, dx, dy, g.n, g.m, p, stream=stream.cuda_stream)
+                    evs[i][1].record(stream)
+            torch.cuda.synchronize(dev)
+        return sum(s_.elapsed_time(e_) for s_, e_ in evs) / a.steps, bool(np.array_equal(dy.cpu().numpy(), want))
+
+    levels = {}
+    for lv in (0, 1):
+        ms_, ok = timed(nps.Params(device=local, level=lv))
+        levels[["warp", "block"][lv]] = {"ms": ms_, "gbs": b_alg / (ms_ * 1e-3) / 1e9, "exact": ok}
+    clk = ClockSampler(local)
+    head = nps.Params(device=local, level=2)
+    ms, exact = timed(head, clk)
+    levels["grid"] = {"ms": ms, "gbs": b_alg / (ms * 1e-3) / 1e9, "exact": exact}
+    peak, peak_src = load_peaks()
+    achieved = b_alg / (ms * 1e-3) / 1e9
+    hg = nps.Graph(g.row_ptr, g.col, np.zeros(0, np.uint32), g.source)
+    pv = torch.from_numpy(val).pin_memory().numpy()
+    px = torch.from_numpy(x).pin_memory().numpy()
+    nps.spmv(hg, pv, px, head)
+    e2e_steps = a.e2e_steps or a.steps
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        y, _ = nps.spmv(hg, pv, px, head)
+    e2e_ms = (time.perf_counter() - t0) / e2e_steps * 1e3
+    cpu = None
+    if rank == 0 and not a.no_cpu_baseline and oracle.have_reference_spmv():
+        yref, _, _, tcpu = oracle.ref_spmv_cpu(g.row_ptr, g.col, 1)
+        cpu = {"value": b_alg / tcpu / 1e9, "unit": "GB/s", "cores": 1, "kind": "reference", "seconds": tcpu,
+               "sample": "one full y = A x by the reference's spmv_omp (SpMV_kernel.cpp:26-42), 1 thread",
+               "exact_vs_gpu": bool(np.array_equal(yref, want) and exact)}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "SpMV GB/s", "value": achieved, "unit": "GB/s", "n_gpus": ws, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(cfg, level="grid", gflops=2 * g.m / (ms * 1e-3) / 1e9, exact_vs_reference=exact,
+                           l2="flushed between steps (256 MB write)", levels=levels),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_source": peak_src, "b_alg_bytes": b_alg,
+                         "b_alg_formula": "12*m + 20*n + 4"},
+            "e2e": {"value": b_alg / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": 4 * (g.n + 1) + 12 * g.m + 8 * g.n, "d2h_bytes_per_step": 8 * g.n,
+                    "exact": bool(np.array_equal(y, want)), "call": "nps.spmv(host arrays, pinned values and x)"},
+            "gpu_launches": 2 * a.steps, "clocks": clk.summary(), "cpu_baseline": cpu}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -711,6 +818,8 @@ def main():
         return bench_solutions(a, nps, ws, rank, local, desc)
     if kind == "bfs":
         return bench_bfs(a, nps, ws, rank, local, desc)
+    if kind == "spmv":
+        return bench_spmv(a, nps, ws, rank, local, desc)
     prm = dict(DEFAULT_PARAMS[kind])
     if a.delta is not None:
         prm["delta"] = a.delta

@@ -28,6 +28,9 @@
  *   nps_bfs                   replaces void bfs_rec_dp_cons_gpu(void), the bfs-rec
  *                             application's consolidated BFS on the same engine
  *                                       apps/bfs-rec/src/gpu/bfs_rec_wrapper.cu:170-229
+ *   nps_spmv                  replaces void spmv_np_consolidate_gpu(void), the SpMV
+ *                             application's consolidated kernel
+ *                                       apps/SpMV/src/gpu/SpMV_wrapper.cu:285-311
  *   nps_degree_stats          replaces the graph analyzer's getStatInfo()
  *                                       utility/graph-analyzer/analyzer.cpp:75-138
  *   nps_graph                 replaces struct _GRAPH_'s CSR members and the
@@ -247,6 +250,19 @@ nps_status nps_sssp_noalloc(const int32_t* d_row_ptr, const int32_t* d_col, cons
 #define NPS_BFS_UNDEFINED 0x7FFFFFFF
 nps_status nps_bfs(const int32_t* row_ptr, const int32_t* col, int32_t n, int64_t m, int32_t src,
                    const nps_params* p, int32_t* level_out, nps_stats* st);
+
+/* ---- sparse matrix-vector product ------------------------------------------
+ * The SpMV application's consolidated kernel (spmv_np_consolidate_gpu,
+ * apps/SpMV/src/gpu/SpMV_wrapper.cu:285-311): y[r] = sum of val[k] * x[col[k]]
+ * over row r of the CSR matrix (row_ptr, col, val), in double precision
+ * (FLOAT_T, apps/SpMV/src/gpu/SpMV.h:13); x and y have n entries.  Rows of at
+ * least p->threshold nonzeros are consolidated at p->level (WARP, BLOCK or GRID;
+ * HYBRID is rejected).  Each y[r] is summed in an order fixed by the matrix, so
+ * results repeat exactly from run to run.  Pointers are host or device per
+ * p->device_ptrs; uses p->device and p->stream.  st (may be NULL) gets
+ * kernel_ms, total_ms, status and grid_ctas. */
+nps_status nps_spmv(const int32_t* row_ptr, const int32_t* col, const double* val, const double* x,
+                    double* y, int32_t n, int64_t m, const nps_params* p, nps_stats* st);
 
 /* ---- the dispatcher's other solutions -------------------------------------
  * SSSP_GPU()'s `solution` switch (apps/sssp/src/gpu/sssp_wrapper.cu:548-583):

@@ -47,7 +47,7 @@ __all__ = [
     "sssp_np_consolidate_gpu", "sssp_solution", "sssp_solution_state", "SolutionInfo",
     "SOLUTION_TQUEUE", "SOLUTION_DUAL_QUEUE", "SOLUTION_SHARED_DELAYED", "SOLUTION_GLOBAL_DELAYED",
     "SOLUTION_NP_NAIVE", "SOLUTION_NP_OPT", "SOLUTION_CONSOLIDATE", "SOLUTION_NAMES", "sssp_batch",
-    "bfs", "bfs_device", "bfs_params", "BFS_UNDEFINED", "trace_read", "fnv1a", "delta_schedule", "degree_stats", "abi_version", "lib",
+    "bfs", "bfs_device", "bfs_params", "BFS_UNDEFINED", "spmv", "spmv_device", "trace_read", "fnv1a", "delta_schedule", "degree_stats", "abi_version", "lib",
 ]
 
 
@@ -344,6 +344,39 @@ def bfs_device(row_ptr, col, n: int, m: int, src: int, level_out, params: Option
     cp = p.to_c(device_ptrs=True, stream=stream)
     check(lib.nps_bfs(_ptr(row_ptr), _ptr(col), n, m, src, C.byref(cp), _ptr(level_out), C.byref(st)),
           "bfs_device")
+    return Stats.from_c(st)
+
+
+def spmv(g: Graph, val, x, params: Optional[Params] = None) -> tuple:
+    """y = A x for the CSR matrix of `g` (row offsets and columns) with values
+    `val` (float64[m]) and x (float64[n]) on host arrays -- the SpMV application's
+    spmv_np_consolidate_gpu() (apps/SpMV/src/gpu/SpMV_wrapper.cu:285-311).  Returns
+    (y float64[n], Stats).  params.level (WARP, BLOCK or GRID, default GRID) and
+    params.threshold select the consolidation of long rows."""
+    p = params or Params(level=CONSOLIDATE_GRID)
+    row = np.ascontiguousarray(g.vertexArray, dtype=np.int32)
+    col = np.ascontiguousarray(g.edgeArray, dtype=np.int32)
+    val = np.ascontiguousarray(val, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    n = g.noNodeTotal
+    if val.shape[0] != col.shape[0] or x.shape[0] != n:
+        raise ValueError("spmv: val needs m entries and x n entries")
+    y = np.empty(n, dtype=np.float64)
+    st = nps_stats()
+    cp = p.to_c(device_ptrs=False)
+    check(lib.nps_spmv(row.ctypes.data, col.ctypes.data, val.ctypes.data, x.ctypes.data, y.ctypes.data, n,
+                       col.shape[0], C.byref(cp), C.byref(st)), "spmv")
+    return y, Stats.from_c(st)
+
+
+def spmv_device(row_ptr, col, val, x, y, n: int, m: int, params: Optional[Params] = None,
+                stream: Optional[int] = None) -> Stats:
+    """spmv() on device-resident arrays (tensors or raw pointers)."""
+    p = params or Params(level=CONSOLIDATE_GRID)
+    st = nps_stats()
+    cp = p.to_c(device_ptrs=True, stream=stream)
+    check(lib.nps_spmv(_ptr(row_ptr), _ptr(col), _ptr(val), _ptr(x), _ptr(y), n, m, C.byref(cp), C.byref(st)),
+          "spmv_device")
     return Stats.from_c(st)
 
 

@@ -10,6 +10,7 @@ in nested-parallelism_b200/ never imports it.
                         from its sources by oracle/Makefile (absent if the
                         reference tree was not available when it was built)
   _ref/libref_bfs.so    the reference's own CPU BFS (bfs-rec's bfs_cpu), likewise
+  _ref/libref_spmv.so   the reference's own CPU SpMV (spmv_omp with its data), likewise
 """
 from __future__ import annotations
 
@@ -23,6 +24,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libref_sssp.so")
 REF_BFS_SO = os.path.join(HERE, "_ref", "libref_bfs.so")
+REF_SPMV_SO = os.path.join(HERE, "_ref", "libref_spmv.so")
 INF = 0x40000000
 BFS_UNDEFINED = 0x7FFFFFFF  # apps/bfs-rec/src/gpu/bfs_rec.h:13
 
@@ -218,6 +220,53 @@ def ref_bfs_cpu(row, col, src):
     level = np.empty(n, dtype=np.int32)
     t = _ref_bfs.nps_ref_bfs_cpu(n, m, row.ctypes.data, col.ctypes.data, int(src), level.ctypes.data)
     return level, float(t)
+
+
+def spmv_data(n, m):
+    """The values and x the reference's SpMV multiplies (prepare_cpu,
+    apps/SpMV/src/cpu/SpMV_kernel.cpp:11-16; the GPU build's prepare_gpu,
+    apps/SpMV/src/gpu/SpMV_wrapper.cu:105-113): val[i] = i % 13 + 0.5 and
+    x[i] = i % 17 + 0.5, in double."""
+    return (np.arange(m) % 13 + 0.5).astype(np.float64), (np.arange(n) % 17 + 0.5).astype(np.float64)
+
+
+def spmv(row, col, val, x):
+    """Restated spmv_omp (apps/SpMV/src/cpu/SpMV_kernel.cpp:26-42): y[r] = sum over
+    row r of val[k] * x[col[k]], accumulated from 0 in k order (bincount adds its
+    weights in index order, the reference's loop order)."""
+    row = np.ascontiguousarray(row, dtype=np.int64)
+    n = row.shape[0] - 1
+    deg = np.diff(row)
+    prod = np.asarray(val, dtype=np.float64) * np.asarray(x, dtype=np.float64)[np.asarray(col, dtype=np.int64)]
+    owner = np.repeat(np.arange(n, dtype=np.int64), deg)
+    return np.bincount(owner, weights=prod, minlength=n).astype(np.float64)
+
+
+def have_reference_spmv() -> bool:
+    return os.path.exists(REF_SPMV_SO)
+
+
+_ref_spmv = None
+
+
+def ref_spmv_cpu(row, col, threads=1):
+    """The reference's SpMV_CPU path on this matrix: its own prepare_cpu() data and
+    spmv_omp() with `threads` OpenMP threads.  Returns (y, x, val, seconds)."""
+    global _ref_spmv
+    if _ref_spmv is None:
+        if not have_reference_spmv():
+            raise ImportError(f"{REF_SPMV_SO} missing: the reference CPU code was not built")
+        lib = C.CDLL(REF_SPMV_SO)
+        lib.nps_ref_spmv_cpu.argtypes = [_I32, _I32, _P, _P, _I32, _P, _P, _P]
+        lib.nps_ref_spmv_cpu.restype = _D
+        _ref_spmv = lib
+    row = np.ascontiguousarray(row, dtype=np.int32)
+    col = np.ascontiguousarray(col, dtype=np.int32)
+    n, m = row.shape[0] - 1, col.shape[0]
+    y, x, val = np.empty(n), np.empty(n), np.empty(max(m, 1))
+    t = _ref_spmv.nps_ref_spmv_cpu(n, m, row.ctypes.data, col.ctypes.data, int(threads), y.ctypes.data,
+                                   x.ctypes.data, val.ctypes.data)
+    return y, x, val[:m], float(t)
 
 
 def degree_stats(row):

@@ -9,7 +9,9 @@ come from the reference's graph analyzer (utility/graph-analyzer/analyzer.cpp),
 built into oracle/_ref/analyzer, run on the reader fixtures and on generated
 graphs written as DIMACS9.  The BFS goldens come from the reference's bfs_cpu
 (apps/bfs-rec/src/gpu/bfs_rec.cpp:100-119), built into oracle/_ref/libref_bfs.so,
-on the same generated graphs and edge cases.  The reader fixtures are small
+on the same generated graphs and edge cases, and the SpMV goldens from the
+reference's SpMV_CPU path (prepare_cpu + spmv_omp, apps/SpMV/src/cpu/
+SpMV_kernel.cpp), built into oracle/_ref/libref_spmv.so.  The reader fixtures are small
 synthetic DIMACS9 / DIMACS10 / SNAP files written here; their expected CSR comes
 from the reference's readInputDIMACS9/10/SLNDC() + convertCSR() (common/
 global.cpp:29-235) on the same files.
@@ -154,6 +156,24 @@ def bfs_goldens():
     return res
 
 
+def spmv_goldens():
+    """y from the reference's spmv_omp on its own data for every case graph (FNV-1a
+    of the float64 bits) and on the edge cases (the values themselves)."""
+    if not oracle.have_reference_spmv():
+        sys.exit("oracle/_ref/libref_spmv.so missing: build it with `make -C oracle` where the reference exists")
+    res = {"cases": {}, "edge_cases": {}}
+    for name, kind, args, _ in CASES:
+        g = gen(kind, args)
+        y, _, _, _ = oracle.ref_spmv_cpu(g.row_ptr, g.col, 1)
+        res["cases"][name] = {"y_fnv1a": oracle.fnv1a(y.view(np.uint32)), "y_sum": float(y.sum()),
+                              "y_max": float(y.max())}
+    for name, n, s, t, w, _ in EDGE_CASES:
+        g = nps.convertCSR(n, s, t, w)
+        y, _, _, _ = oracle.ref_spmv_cpu(g.row_ptr, g.col, 1)
+        res["edge_cases"][name] = [float(v) for v in y]
+    return res
+
+
 def main():
     if not oracle.have_reference():
         sys.exit("oracle/_ref/libref_sssp.so missing: build it with `make -C oracle` where the reference exists")
@@ -185,6 +205,7 @@ def main():
                                  "col_fnv1a": nps.fnv1a(col.view(np.uint32)), "w_fnv1a": nps.fnv1a(w)}
     out["analyzer"] = analyzer_goldens()
     out["bfs"] = bfs_goldens()
+    out["spmv"] = spmv_goldens()
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)
     np.savez_compressed(os.path.join(HERE, "golden_dist.npz"), **dists)
