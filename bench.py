@@ -69,6 +69,9 @@ WORKLOADS = {
     "spmv22": ("spmv", dict(scale=22, edge_factor=16, seed=1000),
                "y = A x in double (the SpMV application's spmv_np_consolidate_gpu) for the R-MAT scale 22, "
                "edge factor 16, seed 1000 matrix with the reference's data: val[i] = i%13+0.5, x[i] = i%17+0.5"),
+    "bc14": ("bc", dict(scale=14, edge_factor=16, seed=1000),
+             "betweenness centrality (the bc application's bc_np_consolidate_gpu) of R-MAT scale 14, edge "
+             "factor 16, seed 1000, every vertex a source in id order, as the reference computes it"),
     "batch64": ("batch", dict(count=64, seed=7),
                 "64 R-MAT instances (a=.57 b=.19 c=.19), scale U{12..18}, edge factor {4,8,16,32}, "
                 "w in [1,255], random sources, seed 7; one persistent CUDA-graph launch per shard"),
@@ -791,6 +794,88 @@ def bench_spmv(a, nps, ws, rank, local, desc):
     return 0
 
 
+def bench_bc(a, nps, ws, rank, local, desc):
+    """Betweenness centrality over every source of the R-MAT scale-14 graph in one
+    nps_bc call per step.  value = source-edges per second (sources x m / device
+    time): each source's forward and backward passes walk the reached rows once
+    each.  Exactness: the first 512 sources against the oracle, bit for bit."""
+    _, args, _ = WORKLOADS[a.workload]
+    g = nps.gen_rmat(args["scale"], args["edge_factor"], seed=args["seed"])
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    cfg = {"workload": a.workload, "description": desc, "n": g.n, "m": g.m, "sources": g.n}
+    sample = np.arange(min(512, g.n))
+    if a.impl == "reference":
+        if rank == 0:
+            # bounded sample: the reference's bc_cpu clears an n x n matrix per source and
+            # takes hours at this size, so the oracle's restatement runs a 512-source sample
+            secs = []
+            for _ in range(a.steps):
+                _, t = oracle.timed(oracle.bc, g.row_ptr, g.col, sample)
+                secs.append(t)
+            value = sample.shape[0] * g.m * a.steps / sum(secs) / 1e9
+            cpu = {"value": value, "unit": "GTEPS", "cores": 1, "kind": "port",
+                   "sample": "the oracle's C restatement of bc_cpu over the first 512 sources per step "
+                             "(the reference's bc_cpu clears an n x n byte matrix per source: hours here)"}
+            print(json.dumps({"impl": "reference", "metric": "BC GTEPS (source-edges/s)", "value": value,
+                              "unit": "GTEPS", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+                              "ms_per_step": 1e3 * sum(secs) / a.steps, "higher_is_better": True,
+                              "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                              "config": dict(cfg, parallelism="host cores", sources=int(sample.shape[0])),
+                              "cpu_baseline": cpu,
+                              "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}))
+        return 0
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    row = torch.from_numpy(g.row_ptr.view(np.int32)).to(dev)
+    col = torch.from_numpy(g.col.view(np.int32)).to(dev)
+    out = torch.empty(g.n, dtype=torch.float32, device=dev)
+    p = nps.Params(device=local)
+    b_sample, _ = nps.bc(g, sample, p)
+    exact = bool(np.array_equal(b_sample.view(np.uint32), oracle.bc(g.row_ptr, g.col, sample).view(np.uint32)))
+    with torch.cuda.stream(stream):
+        for _ in range(a.warmup):
+            nps.bc_device(row, col, g.n, g.m, out, params=p, stream=stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+    clk = ClockSampler(local)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    with clk:
+        with torch.cuda.stream(stream):
+            for i in range(a.steps):
+                evs[i][0].record(stream)
+                st = nps.bc_device(row, col, g.n, g.m, out, params=p, stream=stream.cuda_stream)
+                evs[i][1].record(stream)
+        torch.cuda.synchronize(dev)
+    ms = sum(s_.elapsed_time(e_) for s_, e_ in evs) / a.steps
+    value = g.n * g.m / (ms * 1e-3) / 1e9
+    t0 = time.perf_counter()
+    bh, _ = nps.bc(g, None, p)
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    repeat = bool(np.array_equal(bh.view(np.uint32), out.cpu().numpy().view(np.uint32)))
+    if rank == 0:
+        cpu = None
+        if not a.no_cpu_baseline:
+            _, tcpu = oracle.timed(oracle.bc, g.row_ptr, g.col, sample)
+            cpu = {"value": sample.shape[0] * g.m / tcpu / 1e9, "unit": "GTEPS", "cores": 1, "kind": "port",
+                   "sample": "the oracle's C restatement of bc_cpu over the first 512 sources", "seconds": tcpu}
+        print(json.dumps({
+            "metric": "BC GTEPS (source-edges/s)", "value": value, "unit": "GTEPS", "n_gpus": ws, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(cfg, grid_ctas=st.grid_ctas, exact_first_512_sources=exact,
+                           host_call_matches_device_call=repeat,
+                           l2="the graph (5 MB) stays in L2 across sources; the per-source work is the product"),
+            "roofline": None,
+            "e2e": {"value": g.n * g.m / (e2e_ms * 1e-3) / 1e9, "unit": "GTEPS", "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": 4 * (g.n + 1) + 4 * g.m, "d2h_bytes_per_step": 4 * g.n,
+                    "call": "nps.bc(host Graph)"},
+            "gpu_launches": 3 * a.steps, "clocks": clk.summary(), "cpu_baseline": cpu}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -820,6 +905,8 @@ def main():
         return bench_bfs(a, nps, ws, rank, local, desc)
     if kind == "spmv":
         return bench_spmv(a, nps, ws, rank, local, desc)
+    if kind == "bc":
+        return bench_bc(a, nps, ws, rank, local, desc)
     prm = dict(DEFAULT_PARAMS[kind])
     if a.delta is not None:
         prm["delta"] = a.delta

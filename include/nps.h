@@ -31,6 +31,9 @@
  *   nps_spmv                  replaces void spmv_np_consolidate_gpu(void), the SpMV
  *                             application's consolidated kernel
  *                                       apps/SpMV/src/gpu/SpMV_wrapper.cu:285-311
+ *   nps_bc                    replaces void bc_np_consolidate_gpu(void), the bc
+ *                             application's betweenness centrality
+ *                                       apps/bc/src/gpu/bc_wrapper.cu:678-741
  *   nps_degree_stats          replaces the graph analyzer's getStatInfo()
  *                                       utility/graph-analyzer/analyzer.cpp:75-138
  *   nps_graph                 replaces struct _GRAPH_'s CSR members and the
@@ -108,7 +111,9 @@ typedef struct nps_params {
                                is 2^k wide with k = bits [4b, 4b+4) for b < 7 and bits [28, 32)
                                for every later bucket; delta is then unused (plain policy only) */
   int32_t reserved[3];      /* reserved[0] = 1: test hook, the first in-kernel barrier waits for an
-                               arrival that never comes, so its bounded wait must expire */
+                               arrival that never comes, so its bounded wait must expire.
+                               reserved[1] > 0: nps_bc folds at most this many sources per block
+                               of dependency rows (0 = as many as 2 GB of rows hold) */
 } nps_params;
 
 typedef struct nps_stats {
@@ -263,6 +268,20 @@ nps_status nps_bfs(const int32_t* row_ptr, const int32_t* col, int32_t n, int64_
  * kernel_ms, total_ms, status and grid_ctas. */
 nps_status nps_spmv(const int32_t* row_ptr, const int32_t* col, const double* val, const double* x,
                     double* y, int32_t n, int64_t m, const nps_params* p, nps_stats* st);
+
+/* ---- betweenness centrality -----------------------------------------------
+ * The bc application's consolidated kernels (bc_np_consolidate_gpu,
+ * apps/bc/src/gpu/bc_wrapper.cu:678-741) with the result of its CPU version
+ * bc_cpu (apps/bc/src/cpu/bc.cpp:152-186): Brandes' algorithm over the sources
+ * sources[0..nsrc) in that order (every vertex in id order when sources is
+ * NULL, as the reference does); bc_out[n] receives the float centralities,
+ * bit-identical to bc_cpu for the same source order (a NaN from wrapped path
+ * counts is a NaN on both, with a different payload).  One CTA per source; the
+ * call holds about 16 n bytes per CTA of the grid plus up to 2 GB of per-source
+ * dependency rows.  Pointers (sources included) are host or device per
+ * p->device_ptrs; uses p->device and p->stream. */
+nps_status nps_bc(const int32_t* row_ptr, const int32_t* col, int32_t n, int64_t m, const int32_t* sources,
+                  int32_t nsrc, const nps_params* p, float* bc_out, nps_stats* st);
 
 /* ---- the dispatcher's other solutions -------------------------------------
  * SSSP_GPU()'s `solution` switch (apps/sssp/src/gpu/sssp_wrapper.cu:548-583):

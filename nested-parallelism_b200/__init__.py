@@ -47,7 +47,7 @@ __all__ = [
     "sssp_np_consolidate_gpu", "sssp_solution", "sssp_solution_state", "SolutionInfo",
     "SOLUTION_TQUEUE", "SOLUTION_DUAL_QUEUE", "SOLUTION_SHARED_DELAYED", "SOLUTION_GLOBAL_DELAYED",
     "SOLUTION_NP_NAIVE", "SOLUTION_NP_OPT", "SOLUTION_CONSOLIDATE", "SOLUTION_NAMES", "sssp_batch",
-    "bfs", "bfs_device", "bfs_params", "BFS_UNDEFINED", "spmv", "spmv_device", "trace_read", "fnv1a", "delta_schedule", "degree_stats", "abi_version", "lib",
+    "bfs", "bfs_device", "bfs_params", "BFS_UNDEFINED", "spmv", "spmv_device", "bc", "bc_device", "trace_read", "fnv1a", "delta_schedule", "degree_stats", "abi_version", "lib",
 ]
 
 
@@ -220,6 +220,7 @@ class Params:
     order_degree: int = 0               # delta > 0: rows below this degree ignore the bucket bound
     delta_schedule: int = 0             # per-bucket log2 widths, 4 bits each (see delta_schedule())
     fault_inject_wait: bool = False     # test hook: the first barrier can never complete
+    bc_block_sources: int = 0           # bc: sources per block of dependency rows (0 = as memory allows)
 
     def to_c(self, device_ptrs: bool, stream: Optional[int] = None) -> nps_params:
         p = nps_params()
@@ -236,6 +237,7 @@ class Params:
         p.device_ptrs = int(bool(device_ptrs))
         p.stream = stream
         p.reserved[0] = int(bool(self.fault_inject_wait))
+        p.reserved[1] = int(self.bc_block_sources)
         return p
 
 
@@ -377,6 +379,39 @@ def spmv_device(row_ptr, col, val, x, y, n: int, m: int, params: Optional[Params
     cp = p.to_c(device_ptrs=True, stream=stream)
     check(lib.nps_spmv(_ptr(row_ptr), _ptr(col), _ptr(val), _ptr(x), _ptr(y), n, m, C.byref(cp), C.byref(st)),
           "spmv_device")
+    return Stats.from_c(st)
+
+
+def bc(g: Graph, sources=None, params: Optional[Params] = None) -> tuple:
+    """Betweenness centrality on host arrays -- the bc application's
+    bc_np_consolidate_gpu() (apps/bc/src/gpu/bc_wrapper.cu:678-741) with the
+    exact result of its bc_cpu (apps/bc/src/cpu/bc.cpp:152-186).  `sources` (ints)
+    are taken in the given order; None means every vertex in id order, as the
+    reference does.  Returns (float32 bc, Stats)."""
+    p = params or Params()
+    row = np.ascontiguousarray(g.vertexArray, dtype=np.int32)
+    col = np.ascontiguousarray(g.edgeArray, dtype=np.int32)
+    out = np.empty(g.noNodeTotal, dtype=np.float32)
+    st = nps_stats()
+    cp = p.to_c(device_ptrs=False)
+    if sources is None:
+        srcp, ns = None, 0
+    else:
+        src = np.ascontiguousarray(sources, dtype=np.int32)
+        srcp, ns = src.ctypes.data, src.shape[0]
+    check(lib.nps_bc(row.ctypes.data, col.ctypes.data, g.noNodeTotal, col.shape[0], srcp, ns, C.byref(cp),
+                     out.ctypes.data, C.byref(st)), "bc")
+    return out, Stats.from_c(st)
+
+
+def bc_device(row_ptr, col, n: int, m: int, bc_out, sources=None, nsrc: int = 0,
+              params: Optional[Params] = None, stream: Optional[int] = None) -> Stats:
+    """bc() on device-resident arrays; `sources` is a device array of nsrc ints or None."""
+    p = params or Params()
+    st = nps_stats()
+    cp = p.to_c(device_ptrs=True, stream=stream)
+    check(lib.nps_bc(_ptr(row_ptr), _ptr(col), n, m, None if sources is None else _ptr(sources), nsrc,
+                     C.byref(cp), _ptr(bc_out), C.byref(st)), "bc_device")
     return Stats.from_c(st)
 
 

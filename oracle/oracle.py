@@ -11,6 +11,7 @@ in nested-parallelism_b200/ never imports it.
                         reference tree was not available when it was built)
   _ref/libref_bfs.so    the reference's own CPU BFS (bfs-rec's bfs_cpu), likewise
   _ref/libref_spmv.so   the reference's own CPU SpMV (spmv_omp with its data), likewise
+  _ref/libref_bc.so     the reference's own CPU betweenness centrality (bc_cpu), likewise
 """
 from __future__ import annotations
 
@@ -25,6 +26,7 @@ ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libref_sssp.so")
 REF_BFS_SO = os.path.join(HERE, "_ref", "libref_bfs.so")
 REF_SPMV_SO = os.path.join(HERE, "_ref", "libref_spmv.so")
+REF_BC_SO = os.path.join(HERE, "_ref", "libref_bc.so")
 INF = 0x40000000
 BFS_UNDEFINED = 0x7FFFFFFF  # apps/bfs-rec/src/gpu/bfs_rec.h:13
 
@@ -50,6 +52,8 @@ def _load_oracle():
         lib.oracle_reached.restype = None
         lib.oracle_fnv1a_u32.argtypes = [_P, _I64]
         lib.oracle_fnv1a_u32.restype = C.c_uint64
+        lib.oracle_bc.argtypes = [_I32, _P, _P, _I32, _P, _P]
+        lib.oracle_bc.restype = C.c_int
         _orc = lib
     return _orc
 
@@ -267,6 +271,52 @@ def ref_spmv_cpu(row, col, threads=1):
     t = _ref_spmv.nps_ref_spmv_cpu(n, m, row.ctypes.data, col.ctypes.data, int(threads), y.ctypes.data,
                                    x.ctypes.data, val.ctypes.data)
     return y, x, val[:m], float(t)
+
+
+def bc(row, col, sources=None):
+    """Restated bc_cpu (apps/bc/src/cpu/bc.cpp:152-186, bc_kernel.cpp:3-106):
+    float32 betweenness centrality over `sources` in the given order (every
+    vertex in id order when None), with the reference's float / double rounding
+    step by step (see oracle_bc in sssp_oracle.c)."""
+    row = np.ascontiguousarray(row, dtype=np.int32)
+    col = np.ascontiguousarray(col, dtype=np.int32)
+    n = row.shape[0] - 1
+    out = np.empty(n, dtype=np.float32)
+    if sources is None:
+        rc = _load_oracle().oracle_bc(n, row.ctypes.data, col.ctypes.data, 0, None, out.ctypes.data)
+    else:
+        src = np.ascontiguousarray(sources, dtype=np.int32)
+        rc = _load_oracle().oracle_bc(n, row.ctypes.data, col.ctypes.data, src.shape[0], src.ctypes.data,
+                                      out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("oracle_bc: out of memory")
+    return out
+
+
+def have_reference_bc() -> bool:
+    return os.path.exists(REF_BC_SO)
+
+
+_ref_bc = None
+
+
+def ref_bc_cpu(row, col):
+    """The reference's bc_cpu() over every source (one OpenMP thread; it holds an
+    n x n byte matrix, so only small graphs).  Returns (bc float32, seconds)."""
+    global _ref_bc
+    if _ref_bc is None:
+        if not have_reference_bc():
+            raise ImportError(f"{REF_BC_SO} missing: the reference CPU code was not built")
+        lib = C.CDLL(REF_BC_SO)
+        lib.nps_ref_bc_cpu.argtypes = [_I32, _I32, _P, _P, _P]
+        lib.nps_ref_bc_cpu.restype = _D
+        _ref_bc = lib
+    row = np.ascontiguousarray(row, dtype=np.int32)
+    col = np.ascontiguousarray(col, dtype=np.int32)
+    n = row.shape[0] - 1
+    out = np.empty(n, dtype=np.float32)
+    t = _ref_bc.nps_ref_bc_cpu(n, col.shape[0], row.ctypes.data, col.ctypes.data, out.ctypes.data)
+    return out, float(t)
 
 
 def degree_stats(row):

@@ -22,6 +22,21 @@
  *                      (apps/sssp/src/gpu/sssp_wrapper.cu:475-546 with the
  *                      relaxation of sssp_kernel.cu:49-52), as a FIFO worklist.
  *
+ *   oracle_bc          bc_cpu() of the bc application (apps/bc/src/cpu/bc.cpp:152-186
+ *                      with bc_kernel.cpp:3-106): Brandes betweenness centrality,
+ *                      one source after another.  Forward: a level-synchronous BFS
+ *                      from the source counting shortest paths, sigma[v] += sigma[u]
+ *                      for every edge u -> v with level[v] = level[u] + 1
+ *                      (bc_kernel.cpp:29-49; int sums, wrapping like the reference's
+ *                      __sync_fetch_and_add).  Backward, deepest level first: for u at
+ *                      level L, over its edges in CSR order to v at level L + 1,
+ *                      delta[u] = (float)((double)delta[u] + (double)sigma[u] /
+ *                      sigma[v] * (1.0f + delta[v])) -- the reference's p[u][v] = 1 is
+ *                      exactly "edge u -> v and level[v] = level[u] + 1"
+ *                      (bc_kernel.cpp:51-64); then bc[v] += delta[v] in float for every
+ *                      reached v other than the source (:83-101).  MAX_LEVEL = 9999
+ *                      marks unvisited vertices, as in common/global.h:17.
+ *
  * Distances are uint32 with INF = 2^30 (sssp_wrapper.cu:7, common/global.h:19).
  * A tentative distance that reaches 2^30 is treated as unreachable; the
  * reference's int arithmetic never gets there on the inputs it is run on.
@@ -266,4 +281,78 @@ uint64_t oracle_fnv1a_u32(const uint32_t* a, int64_t n) {
   uint64_t h = 1469598103934665603ull;
   for (int64_t i = 0; i < n; ++i) h = (h ^ (uint64_t)a[i]) * 1099511628211ull;
   return h;
+}
+
+/* Betweenness centrality of every vertex over the sources in `sources` (all
+ * vertices in id order when sources is NULL), as bc_cpu() accumulates it; see
+ * the header for the steps.  bc[n] is overwritten.  Returns 0, or -1 when out of
+ * memory. */
+#define ORACLE_MAX_LEVEL 9999
+int oracle_bc(int32_t n, const int32_t* row, const int32_t* col, int32_t nsrc, const int32_t* sources,
+              float* bc) {
+  int32_t* level = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
+  int32_t* sigma = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
+  float* delta = (float*)malloc(sizeof(float) * (size_t)n);
+  int32_t* order = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
+  int32_t* lb = (int32_t*)malloc(sizeof(int32_t) * ((size_t)n + 2));
+  if (!level || !sigma || !delta || !order || !lb) {
+    free(level), free(sigma), free(delta), free(order), free(lb);
+    return -1;
+  }
+  for (int32_t v = 0; v < n; ++v) {
+    bc[v] = 0.0f;
+    level[v] = ORACLE_MAX_LEVEL;
+    sigma[v] = 0;
+    delta[v] = 0.0f;
+  }
+  const int32_t count = sources ? nsrc : n;
+  for (int32_t k = 0; k < count; ++k) {
+    const int32_t s = sources ? sources[k] : k;
+    int32_t tail = 0, dist = 0;
+    level[s] = 0;
+    sigma[s] = 1;
+    order[tail++] = s;
+    lb[0] = 0;
+    lb[1] = 1;
+    /* forward: frontier = the vertices of level `dist` */
+    while (lb[dist] < lb[dist + 1]) {
+      for (int32_t i = lb[dist]; i < lb[dist + 1]; ++i) {
+        const int32_t u = order[i];
+        for (int32_t e = row[u]; e < row[u + 1]; ++e) {
+          const int32_t v = col[e];
+          if (level[v] == ORACLE_MAX_LEVEL) {
+            level[v] = dist + 1;
+            order[tail++] = v;
+          }
+          if (level[v] == dist + 1) sigma[v] = (int32_t)((uint32_t)sigma[v] + (uint32_t)sigma[u]);
+        }
+      }
+      lb[dist + 2] = tail;
+      ++dist;
+    }
+    /* here dist = deepest level + 1, as the reference's loop leaves it */
+    for (int32_t d = dist; d > 1; --d) {
+      for (int32_t i = lb[d - 2]; i < lb[d - 1]; ++i) { /* u at level d - 2 */
+        const int32_t u = order[i];
+        float du = delta[u];
+        for (int32_t e = row[u]; e < row[u + 1]; ++e) {
+          const int32_t v = col[e];
+          if (level[v] == d - 1) du = (float)((double)du + (double)sigma[u] / (double)sigma[v] * (double)(1.0f + delta[v]));
+        }
+        delta[u] = du;
+      }
+      for (int32_t i = lb[d - 1]; i < lb[d]; ++i) { /* v at level d - 1 */
+        const int32_t v = order[i];
+        if (v != s) bc[v] = bc[v] + delta[v];
+      }
+    }
+    for (int32_t i = 0; i < tail; ++i) {
+      const int32_t v = order[i];
+      level[v] = ORACLE_MAX_LEVEL;
+      sigma[v] = 0;
+      delta[v] = 0.0f;
+    }
+  }
+  free(level), free(sigma), free(delta), free(order), free(lb);
+  return 0;
 }

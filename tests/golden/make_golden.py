@@ -11,7 +11,10 @@ graphs written as DIMACS9.  The BFS goldens come from the reference's bfs_cpu
 (apps/bfs-rec/src/gpu/bfs_rec.cpp:100-119), built into oracle/_ref/libref_bfs.so,
 on the same generated graphs and edge cases, and the SpMV goldens from the
 reference's SpMV_CPU path (prepare_cpu + spmv_omp, apps/SpMV/src/cpu/
-SpMV_kernel.cpp), built into oracle/_ref/libref_spmv.so.  The reader fixtures are small
+SpMV_kernel.cpp), built into oracle/_ref/libref_spmv.so, and the betweenness
+centrality goldens from the reference's bc_cpu (apps/bc/src/cpu/bc.cpp), built
+into oracle/_ref/libref_bc.so, on small graphs (it keeps an n x n matrix).  The
+reader fixtures are small
 synthetic DIMACS9 / DIMACS10 / SNAP files written here; their expected CSR comes
 from the reference's readInputDIMACS9/10/SLNDC() + convertCSR() (common/
 global.cpp:29-235) on the same files.
@@ -174,6 +177,31 @@ def spmv_goldens():
     return res
 
 
+# graphs small enough for the reference's bc_cpu, which clears an n x n byte matrix per source
+BC_GRAPHS = [("rmat10_ef8_s3", "rmat", dict(scale=10, edge_factor=8, seed=3)),
+             ("rmat11_ef16_s7", "rmat", dict(scale=11, edge_factor=16, seed=7)),
+             ("grid30_s1", "grid", dict(rows=30, cols=30, drop=0.1, wmax=10, seed=1)),
+             ("uniform1500_s2", "uniform", dict(n=1500, m=6000, wmax=10, seed=2))]
+
+
+def bc_goldens():
+    """Centralities from the reference's bc_cpu (every vertex a source, one thread):
+    FNV-1a of the float32 bits per graph, and the values for the edge cases."""
+    if not oracle.have_reference_bc():
+        sys.exit("oracle/_ref/libref_bc.so missing: build it with `make -C oracle` where the reference exists")
+    res = {"cases": {}, "edge_cases": {}}
+    for name, kind, args in BC_GRAPHS:
+        g = gen(kind, args)
+        b, _ = oracle.ref_bc_cpu(g.row_ptr, g.col)
+        res["cases"][name] = {"kind": kind, "args": args, "bc_fnv1a": oracle.fnv1a(b.view(np.uint32)),
+                              "bc_max": float(b.max()), "bc_sum": float(b.astype(np.float64).sum())}
+    for name, n, s, t, w, _ in EDGE_CASES:
+        g = nps.convertCSR(n, s, t, w)
+        b, _ = oracle.ref_bc_cpu(g.row_ptr, g.col)
+        res["edge_cases"][name] = [float(v) for v in b]
+    return res
+
+
 def main():
     if not oracle.have_reference():
         sys.exit("oracle/_ref/libref_sssp.so missing: build it with `make -C oracle` where the reference exists")
@@ -206,6 +234,7 @@ def main():
     out["analyzer"] = analyzer_goldens()
     out["bfs"] = bfs_goldens()
     out["spmv"] = spmv_goldens()
+    out["bc"] = bc_goldens()
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)
     np.savez_compressed(os.path.join(HERE, "golden_dist.npz"), **dists)
