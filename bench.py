@@ -72,6 +72,9 @@ WORKLOADS = {
     "bc14": ("bc", dict(scale=14, edge_factor=16, seed=1000),
              "betweenness centrality (the bc application's bc_np_consolidate_gpu) of R-MAT scale 14, edge "
              "factor 16, seed 1000, every vertex a source in id order, as the reference computes it"),
+    "color22": ("color", dict(scale=22, edge_factor=16, seed=1000),
+                "graph coloring (the graph-color application's gclr_np_consolidate_gpu) of R-MAT scale 22, "
+                "edge factor 16, seed 1000 (1,295 colors, so 1,295 reference iterations)"),
     "batch64": ("batch", dict(count=64, seed=7),
                 "64 R-MAT instances (a=.57 b=.19 c=.19), scale U{12..18}, edge factor {4,8,16,32}, "
                 "w in [1,255], random sources, seed 7; one persistent CUDA-graph launch per shard"),
@@ -876,6 +879,75 @@ def bench_bc(a, nps, ws, rank, local, desc):
     return 0
 
 
+def bench_color(a, nps, ws, rank, local, desc):
+    """Graph coloring of the R-MAT scale-22 graph, device arrays resident, colors
+    compared exactly with the oracle.  value = edges / device time (each edge is
+    read about once by the resumable scan)."""
+    _, args, _ = WORKLOADS[a.workload]
+    g = nps.gen_rmat(args["scale"], args["edge_factor"], seed=args["seed"])
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    cfg = {"workload": a.workload, "description": desc, "n": g.n, "m": g.m}
+    if a.impl == "reference":
+        if rank == 0:
+            secs = [oracle.timed(oracle.color, g.row_ptr, g.col)[1] for _ in range(a.steps)]
+            value = g.m * a.steps / sum(secs) / 1e9
+            cpu = {"value": value, "unit": "GTEPS", "cores": 1, "kind": "port",
+                   "sample": "the oracle's closed form in id order (C), one full coloring per step; the "
+                             "reference has no CPU coloring and its iterations would take n x colors steps"}
+            print(json.dumps({"impl": "reference", "metric": "coloring GTEPS", "value": value, "unit": "GTEPS",
+                              "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+                              "ms_per_step": 1e3 * sum(secs) / a.steps, "higher_is_better": True,
+                              "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+                              "config": dict(cfg, parallelism="host cores"), "cpu_baseline": cpu,
+                              "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}))
+        return 0
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    row = torch.from_numpy(g.row_ptr.view(np.int32)).to(dev)
+    col = torch.from_numpy(g.col.view(np.int32)).to(dev)
+    out = torch.empty(g.n, dtype=torch.int32, device=dev)
+    want, iters = oracle.color(g.row_ptr, g.col)
+    p = nps.Params(device=local)
+    with torch.cuda.stream(stream):
+        for _ in range(a.warmup):
+            nps.color_device(row, col, g.n, g.m, out, p, stream=stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+    clk = ClockSampler(local)
+    ms_l = []
+    with clk:
+        for _ in range(a.steps):
+            st = nps.color_device(row, col, g.n, g.m, out, p, stream=stream.cuda_stream)
+            ms_l.append(st.kernel_ms)
+    exact = bool(np.array_equal(out.cpu().numpy(), want))
+    ms = sum(ms_l) / a.steps
+    t0 = time.perf_counter()
+    got, _ = nps.color(g, p)
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    if rank == 0:
+        cpu = None
+        if not a.no_cpu_baseline:
+            _, tcpu = oracle.timed(oracle.color, g.row_ptr, g.col)
+            cpu = {"value": g.m / tcpu / 1e9, "unit": "GTEPS", "cores": 1, "kind": "port", "seconds": tcpu,
+                   "sample": "the oracle's closed form in id order (C), one full coloring"}
+        print(json.dumps({
+            "metric": "coloring GTEPS", "value": g.m / (ms * 1e-3) / 1e9, "unit": "GTEPS", "n_gpus": ws,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": dict(cfg, colors=iters, rounds=st.buckets, edges_scanned=st.edges_scanned,
+                           exact_vs_oracle=exact, iterations_match=st.iterations == iters,
+                           timing="CUDA events around the call's rounds (host reads the list once per chunk)"),
+            "roofline": None,
+            "e2e": {"value": g.m / (e2e_ms * 1e-3) / 1e9, "unit": "GTEPS", "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": 4 * (g.n + 1) + 4 * g.m, "d2h_bytes_per_step": 4 * g.n,
+                    "exact": bool(np.array_equal(got, want)), "call": "nps.color(host Graph)"},
+            "gpu_launches": 1 + st.buckets, "clocks": clk.summary(), "cpu_baseline": cpu}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -907,6 +979,8 @@ def main():
         return bench_spmv(a, nps, ws, rank, local, desc)
     if kind == "bc":
         return bench_bc(a, nps, ws, rank, local, desc)
+    if kind == "color":
+        return bench_color(a, nps, ws, rank, local, desc)
     prm = dict(DEFAULT_PARAMS[kind])
     if a.delta is not None:
         prm["delta"] = a.delta

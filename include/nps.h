@@ -34,6 +34,9 @@
  *   nps_bc                    replaces void bc_np_consolidate_gpu(void), the bc
  *                             application's betweenness centrality
  *                                       apps/bc/src/gpu/bc_wrapper.cu:678-741
+ *   nps_color                 replaces void gclr_np_consolidate_gpu(void), the
+ *                             graph-color application's coloring
+ *                                       apps/graph-color/src/gpu/graph_color_wrapper.cu:368-412
  *   nps_degree_stats          replaces the graph analyzer's getStatInfo()
  *                                       utility/graph-analyzer/analyzer.cpp:75-138
  *   nps_graph                 replaces struct _GRAPH_'s CSR members and the
@@ -282,6 +285,17 @@ nps_status nps_spmv(const int32_t* row_ptr, const int32_t* col, const double* va
  * p->device_ptrs; uses p->device and p->stream. */
 nps_status nps_bc(const int32_t* row_ptr, const int32_t* col, int32_t n, int64_t m, const int32_t* sources,
                   int32_t nsrc, const nps_params* p, float* bc_out, nps_stats* st);
+
+/* ---- graph coloring ---------------------------------------------------------
+ * The graph-color application's consolidated coloring (gclr_np_consolidate_gpu,
+ * apps/graph-color/src/gpu/graph_color_wrapper.cu:368-412): color_out[n]
+ * receives the colors the reference's iterations assign, color(v) = 1 + the
+ * largest color among v's out-neighbours with a smaller id (1 when there is
+ * none); st->iterations = the largest color (the reference's iteration count).
+ * Rows of at least p->threshold edges are scanned by a warp.  Pointers are host
+ * or device per p->device_ptrs; uses p->device, p->stream and p->timeout_s. */
+nps_status nps_color(const int32_t* row_ptr, const int32_t* col, int32_t n, int64_t m, const nps_params* p,
+                     int32_t* color_out, nps_stats* st);
 
 /* ---- the dispatcher's other solutions -------------------------------------
  * SSSP_GPU()'s `solution` switch (apps/sssp/src/gpu/sssp_wrapper.cu:548-583):

@@ -47,7 +47,7 @@ __all__ = [
     "sssp_np_consolidate_gpu", "sssp_solution", "sssp_solution_state", "SolutionInfo",
     "SOLUTION_TQUEUE", "SOLUTION_DUAL_QUEUE", "SOLUTION_SHARED_DELAYED", "SOLUTION_GLOBAL_DELAYED",
     "SOLUTION_NP_NAIVE", "SOLUTION_NP_OPT", "SOLUTION_CONSOLIDATE", "SOLUTION_NAMES", "sssp_batch",
-    "bfs", "bfs_device", "bfs_params", "BFS_UNDEFINED", "spmv", "spmv_device", "bc", "bc_device", "trace_read", "fnv1a", "delta_schedule", "degree_stats", "abi_version", "lib",
+    "bfs", "bfs_device", "bfs_params", "BFS_UNDEFINED", "spmv", "spmv_device", "bc", "bc_device", "color", "color_device", "trace_read", "fnv1a", "delta_schedule", "degree_stats", "abi_version", "lib",
 ]
 
 
@@ -379,6 +379,32 @@ def spmv_device(row_ptr, col, val, x, y, n: int, m: int, params: Optional[Params
     cp = p.to_c(device_ptrs=True, stream=stream)
     check(lib.nps_spmv(_ptr(row_ptr), _ptr(col), _ptr(val), _ptr(x), _ptr(y), n, m, C.byref(cp), C.byref(st)),
           "spmv_device")
+    return Stats.from_c(st)
+
+
+def color(g: Graph, params: Optional[Params] = None) -> tuple:
+    """Graph coloring on host arrays -- the graph-color application's
+    gclr_np_consolidate_gpu() (apps/graph-color/src/gpu/graph_color_wrapper.cu:368-412).
+    Returns (int32 colors, Stats); Stats.iterations is the reference's iteration
+    count (the largest color)."""
+    p = params or Params()
+    row = np.ascontiguousarray(g.vertexArray, dtype=np.int32)
+    col = np.ascontiguousarray(g.edgeArray, dtype=np.int32)
+    out = np.empty(g.noNodeTotal, dtype=np.int32)
+    st = nps_stats()
+    cp = p.to_c(device_ptrs=False)
+    check(lib.nps_color(row.ctypes.data, col.ctypes.data, g.noNodeTotal, col.shape[0], C.byref(cp), out.ctypes.data,
+                        C.byref(st)), "color")
+    return out, Stats.from_c(st)
+
+
+def color_device(row_ptr, col, n: int, m: int, color_out, params: Optional[Params] = None,
+                 stream: Optional[int] = None) -> Stats:
+    """color() on device-resident arrays, as the reference leaves d_colorArray."""
+    p = params or Params()
+    st = nps_stats()
+    cp = p.to_c(device_ptrs=True, stream=stream)
+    check(lib.nps_color(_ptr(row_ptr), _ptr(col), n, m, C.byref(cp), _ptr(color_out), C.byref(st)), "color_device")
     return Stats.from_c(st)
 
 

@@ -113,6 +113,7 @@ SIGNATURES = {
                             C.POINTER(nps_stats)]),
     "nps_sssp_state": (_I32, [_P, _P, _P, _I32, _I64, _P, _P, C.POINTER(nps_params),
                               C.POINTER(nps_stats)]),
+    "nps_color": (_I32, [_P, _P, _I32, _I64, C.POINTER(nps_params), _P, C.POINTER(nps_stats)]),
     "nps_bc": (_I32, [_P, _P, _I32, _I64, _P, _I32, C.POINTER(nps_params), _P, C.POINTER(nps_stats)]),
     "nps_spmv": (_I32, [_P, _P, _P, _P, _P, _I32, _I64, C.POINTER(nps_params), C.POINTER(nps_stats)]),
     "nps_bfs": (_I32, [_P, _P, _I32, _I64, _I32, C.POINTER(nps_params), _P, C.POINTER(nps_stats)]),

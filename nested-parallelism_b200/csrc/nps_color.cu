@@ -1,0 +1,528 @@
+// Graph coloring: the graph-color application (gclr_np_consolidate_gpu,
+// apps/graph-color/src/gpu/graph_color_wrapper.cu:368-412, kernels
+// graph_color_kernel.cu:14-35 and :541-723).
+//
+// The reference colors in iterations c = 1, 2, ...: an uncolored vertex v takes
+// color c when none of its out-neighbours u < v is uncolored or colored c
+// (graph_color_kernel.cu:19-32); it stops when every vertex is colored.  A
+// neighbour that takes color c in the same iteration blocks v whether v sees it
+// before or after, so the result does not depend on scheduling:
+//     color(v) = 1 + max { color(u) : u in the row of v, u < v }
+// (1 when v has no smaller out-neighbour), and the iteration count is the
+// largest color.  The reference tests every uncolored vertex in every iteration.
+//
+// Here the same colors come from a dependency count per vertex, reading every
+// edge twice in all:
+//   1. pending[v] = the edges of v's row to smaller vertices; the reverse lists
+//      (for every u, the vertices v > u whose rows hold u) are built by a count,
+//      an exclusive scan and a scatter.
+//   2. Vertices with pending = 0 take color 1 and form the first frontier.
+//   3. A round walks the reverse lists of the frontier: for each dependant w,
+//      best[w] = max(best[w], color(v)), a fence, then pending[w] -= 1; the
+//      update that takes pending to 0 gives w the color best + 1 and puts it
+//      on the next frontier.  A round per color,
+//      each touching only that color's vertices and their reverse lists.
+// Rows of at least `threshold` entries are walked by a whole warp when the
+// dependency counts are built, shorter ones by one thread.  In a round, a warp
+// walks the reverse lists of 32 frontier vertices flat, 32 entries per step, and
+// reverse lists of kHuge entries or more (the hubs: vertex 0 of an R-MAT graph
+// has millions of dependants) are cut into chunks that a second kernel of the
+// round spreads over every warp -- the warp / grid consolidation of long rows.  Rounds are
+// enqueued in chunks and the host reads the frontier length once per chunk, as
+// for the SSSP solutions 0-5.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "nps.h"
+#include "nps_internal.h"
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kScanItems = 1024;  // elements per CTA of the scan (4 per thread)
+constexpr int kMaxChunk = 32;      // rounds per host read-back, at most
+constexpr int32_t kHuge = 256;     // reverse lists this long are cut into chunks for all warps
+constexpr int32_t kChunk = 256;    // entries per chunk
+constexpr unsigned kFull = 0xffffffffu;
+
+struct ColorCtr {
+  uint32_t len[3];   // frontier of round r in len[r % 3]; round r zeroes len[(r + 2) % 3],
+                     // which round r - 1 read and round r + 1 fills
+  uint32_t chunks[3];  // chunks of huge reverse lists of round r in chunks[r % 3]
+  uint32_t status;
+  uint32_t rounds;   // rounds whose frontier was not empty
+  int32_t max_color;
+  uint32_t left;     // uncolored vertices at the end (0 unless the input is malformed)
+  uint32_t pad;
+  unsigned long long edges;
+};
+
+struct ColorArgs {
+  const int32_t* row;
+  const int32_t* col;
+  int32_t n;
+  int64_t m;
+  int32_t* color;
+  int32_t* pending;  // per vertex: edges to smaller vertices not yet colored
+  int32_t* best;     // per vertex: the largest color among those colored so far
+  int32_t* rrow;     // n + 1 reverse-list offsets (first the per-vertex counts)
+  int32_t* rcur;     // scatter cursors
+  int32_t* rcol;     // reverse lists
+  int32_t* bsum;     // scan: one total per scan CTA
+  int32_t* list[2];  // frontiers by round parity
+  int4* chunk;       // this round's chunks of huge reverse lists
+  int32_t threshold;
+  ColorCtr* c;
+};
+
+__device__ __forceinline__ void flag_format(ColorCtr* c) { atomicCAS(&c->status, 0u, (uint32_t)NPS_ERR_FORMAT); }
+
+// Calls f(v, k) for every edge k of every row v in [0, n): a thread per row
+// below `threshold` edges, a warp per longer row (all lanes of a warp take part;
+// rows are swept warp by warp).
+template <class F>
+__device__ __forceinline__ void for_each_edge(const ColorArgs& a, F f) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (kThreads / 32);
+  for (int64_t base = ((int64_t)blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)) * 32; base < a.n;
+       base += warps * 32) {
+    const int64_t v = base + lane;
+    int32_t s = 0, e = 0;
+    if (v < a.n) {
+      s = a.row[v];
+      e = a.row[v + 1];
+      if (s < 0 || e < s || (int64_t)e > a.m) {
+        flag_format(a.c);
+        s = e = 0;
+      }
+    }
+    const bool large = e - s >= a.threshold;
+    if (!large)
+      for (int32_t k = s; k < e; ++k) f((int32_t)v, k);
+    unsigned lm = __ballot_sync(kFull, large);
+    while (lm) {
+      const int j = __ffs(lm) - 1;
+      lm &= lm - 1;
+      const int32_t jv = __shfl_sync(kFull, (int32_t)v, j);
+      const int32_t js = __shfl_sync(kFull, s, j), je = __shfl_sync(kFull, e, j);
+      for (int32_t k = js + lane; k < je; k += 32) f(jv, k);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) color_count_kernel(ColorArgs a) {
+  for_each_edge(a, [&](int32_t v, int32_t k) {
+    const int32_t u = a.col[k];
+    if ((uint32_t)u >= (uint32_t)a.n) {
+      flag_format(a.c);
+    } else if (u < v) {
+      atomicAdd(a.pending + v, 1);
+      atomicAdd(a.rrow + u, 1);
+    }
+  });
+}
+
+// Exclusive scan of rrow[0, n) in place, rrow[n] = total: per-CTA scans of
+// kScanItems, a single CTA over the CTA totals, then the offsets added.
+__global__ void __launch_bounds__(kThreads) scan_blocks_kernel(int32_t* x, int32_t n, int32_t* bsum) {
+  __shared__ int32_t s_warp[kThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t base = (int64_t)blockIdx.x * kScanItems + threadIdx.x * 4;
+  int32_t v[4], t = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    v[i] = base + i < n ? x[base + i] : 0;
+    t += v[i];
+  }
+  int32_t incl = t;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int32_t y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) s_warp[warp] = incl;
+  __syncthreads();
+  int32_t woff = 0;
+  for (int w = 0; w < warp; ++w) woff += s_warp[w];
+  int32_t run = woff + incl - t;  // exclusive prefix of this thread's first element within the CTA
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    if (base + i < n) x[base + i] = run;
+    run += v[i];
+  }
+  if (threadIdx.x == kThreads - 1) bsum[blockIdx.x] = woff + incl;
+}
+
+__global__ void __launch_bounds__(kThreads) scan_totals_kernel(int32_t* bsum, int32_t nb, int32_t* total) {
+  __shared__ int32_t s_carry;
+  __shared__ int32_t s_warp[kThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (int32_t base = 0; base < nb; base += kThreads) {
+    const int32_t i = base + threadIdx.x;
+    const int32_t t = i < nb ? bsum[i] : 0;
+    int32_t incl = t;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int32_t y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    int32_t woff = 0;
+    for (int w = 0; w < warp; ++w) woff += s_warp[w];
+    if (i < nb) bsum[i] = s_carry + woff + incl - t;
+    __syncthreads();
+    if (threadIdx.x == kThreads - 1) s_carry += woff + incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = s_carry;
+}
+
+__global__ void scan_add_kernel(int32_t* x, int32_t n, const int32_t* bsum, int32_t* cur) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t y = x[i] + bsum[i / kScanItems];
+    x[i] = y;
+    cur[i] = y;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) color_scatter_kernel(ColorArgs a) {
+  for_each_edge(a, [&](int32_t v, int32_t k) {
+    const int32_t u = a.col[k];
+    if ((uint32_t)u < (uint32_t)a.n && u < v) a.rcol[atomicAdd(a.rcur + u, 1)] = v;
+  });
+}
+
+// Vertices without smaller out-neighbours take color 1: the first frontier.
+__global__ void color_first_kernel(ColorArgs a) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < a.n; v += (int64_t)gridDim.x * blockDim.x) {
+    const bool ready = a.pending[v] == 0;
+    a.color[v] = ready ? 1 : 0;
+    if (ready) a.list[0][atomicAdd(&a.c->len[0], 1u)] = (int32_t)v;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(&a.c->max_color, 1);  // vertex 0 is always ready
+}
+
+// One dependant w of a vertex of color cv: best[w] rises to cv, a fence orders
+// that before the decrement of pending[w], and the decrement that takes it to
+// 0 (after a second fence) reads best and colors w with best + 1.  Returns the
+// color given (0 when w is still waiting).
+__device__ __forceinline__ int32_t settle(const ColorArgs& a, int32_t w, int32_t cv, int32_t* out, uint32_t* len) {
+  atomicMax(a.best + w, cv);
+  __threadfence();
+  if (atomicSub(a.pending + w, 1) != 1) return 0;
+  __threadfence();
+  const int32_t cw = __ldcg(a.best + w) + 1;
+  a.color[w] = cw;
+  out[atomicAdd(len, 1u)] = w;
+  return cw;
+}
+
+// Round r (r3 = r % 3, par = r & 1): walk the reverse lists of frontier list[par].
+// A warp takes 32 frontier vertices and walks their reverse lists flat, 32
+// entries per step (a 5-step shuffle search finds each entry's vertex), so the
+// longest chain of dependent atomics in a warp is its lists' total / 32.  Lists
+// of kHuge entries or more are cut into kChunk pieces for color_chunks_kernel,
+// which runs next and spreads them over every warp.
+__global__ void __launch_bounds__(kThreads) color_round_kernel(ColorArgs a, int r3, int par) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.c->len[(r3 + 2) % 3] = 0;
+    a.c->chunks[(r3 + 2) % 3] = 0;
+  }
+  const uint32_t len = a.c->len[r3];
+  if (len == 0) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) a.c->rounds += 1;
+  const int lane = threadIdx.x & 31;
+  const int32_t* in = a.list[par];
+  int32_t* out = a.list[par ^ 1];
+  uint32_t* out_len = &a.c->len[(r3 + 1) % 3];
+  int32_t most = 0;
+  unsigned long long edges = 0;
+  const uint32_t warps = gridDim.x * (kThreads / 32);
+  for (uint32_t base = (blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)) * 32u; base < len; base += warps * 32u) {
+    const uint32_t i = base + lane;
+    int32_t v = -1, s = 0, e = 0, cv = 0;
+    if (i < len) {
+      v = in[i];
+      s = a.rrow[v];
+      e = a.rrow[v + 1];
+      cv = a.color[v];
+      edges += e - s;
+    }
+    const int32_t d = e - s;
+    const bool huge = d >= kHuge;
+    const uint32_t flat = huge ? 0u : (uint32_t)d;
+    uint32_t incl = flat;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const uint32_t excl = incl - flat, total = __shfl_sync(kFull, incl, 31);
+    for (uint32_t fb = 0; fb < total; fb += 32) {
+      const uint32_t k = fb + lane;
+      int o = 0;  // the last lane whose prefix is <= k
+#pragma unroll
+      for (int step = 16; step >= 1; step >>= 1) {
+        const uint32_t x = __shfl_sync(kFull, excl, o + step);
+        if (x <= k) o += step;
+      }
+      const int32_t os = __shfl_sync(kFull, s, o), oc = __shfl_sync(kFull, cv, o);
+      const uint32_t oe = __shfl_sync(kFull, excl, o);
+      if (k < total) most = max(most, settle(a, a.rcol[os + (int32_t)(k - oe)], oc, out, out_len));
+    }
+    // huge lists: one chunk descriptor per kChunk entries, reserved once per warp
+    const uint32_t nch = huge ? (uint32_t)((d + kChunk - 1) / kChunk) : 0u;
+    uint32_t cincl = nch;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(kFull, cincl, o);
+      if (lane >= o) cincl += t;
+    }
+    const uint32_t ctot = __shfl_sync(kFull, cincl, 31);
+    if (ctot) {
+      uint32_t cb = 0;
+      if (lane == 31) cb = atomicAdd(&a.c->chunks[r3], ctot);
+      cb = __shfl_sync(kFull, cb, 31) + (cincl - nch);
+      for (uint32_t q = 0; q < nch; ++q) {
+        const int32_t cs = s + (int32_t)q * kChunk;
+        a.chunk[cb + q] = make_int4(v, cs, min(e, cs + kChunk), cv);
+      }
+    }
+  }
+  const unsigned long long we = __reduce_add_sync(kFull, (unsigned)min(edges, 0xffffffffull));
+  most = __reduce_max_sync(kFull, most);
+  if (lane == 0) {
+    if (we) atomicAdd(&a.c->edges, we);
+    if (most) atomicMax(&a.c->max_color, most);
+  }
+}
+
+// The same round, second pass: one warp per chunk of a huge reverse list.
+__global__ void __launch_bounds__(kThreads) color_chunks_kernel(ColorArgs a, int r3, int par) {
+  const uint32_t nc = a.c->chunks[r3];
+  if (nc == 0) return;
+  const int lane = threadIdx.x & 31;
+  int32_t* out = a.list[par ^ 1];
+  uint32_t* out_len = &a.c->len[(r3 + 1) % 3];
+  int32_t most = 0;
+  const uint32_t warps = gridDim.x * (kThreads / 32);
+  for (uint32_t q = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5); q < nc; q += warps) {
+    const int4 cd = a.chunk[q];  // {vertex, first, end, its color}
+    for (int32_t k = cd.y + lane; k < cd.z; k += 32) most = max(most, settle(a, a.rcol[k], cd.w, out, out_len));
+  }
+  most = __reduce_max_sync(kFull, most);
+  if (lane == 0 && most) atomicMax(&a.c->max_color, most);
+}
+
+__global__ void color_left_kernel(const int32_t* color, int32_t n, uint32_t* left) {
+  uint32_t c = 0;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+    c += color[v] == 0;
+  c = __reduce_add_sync(kFull, c);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(left, c);
+}
+
+#define CL_CUDA(call)                                                                         \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess)                                                                    \
+      return nps_fail(NPS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
+  } while (0)
+
+struct ColorWork {
+  std::mutex mu;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[4] = {};
+  cudaEvent_t chunk_ev[2] = {};
+  int sms = 0;
+  ColorCtr* ctr = nullptr;
+  ColorCtr* snap = nullptr;  // pinned: [0], [1] per chunk, [2] final
+  int32_t* buf = nullptr;    // rrow, rcur, list 0, list 1, scan totals
+  size_t buf_n = 0;
+  int32_t* state = nullptr;  // pending, best
+  size_t state_n = 0;
+  int4* chunk = nullptr;
+  size_t chunk_n = 0;
+  int32_t* rcol = nullptr;
+  size_t rcol_n = 0;
+  int32_t* row = nullptr;
+  size_t row_n = 0;
+  int32_t* col = nullptr;
+  size_t col_n = 0;
+  int32_t* color = nullptr;
+  size_t color_n = 0;
+};
+
+std::mutex g_color_mu;
+std::vector<ColorWork*> g_color;
+
+template <class T>
+nps_status ensure(T** p, size_t* have, size_t want, cudaStream_t s) {
+  if (*p && *have >= want) return NPS_OK;
+  if (*p) {
+    cudaStreamSynchronize(s);
+    cudaFree(*p);
+  }
+  *p = nullptr;
+  *have = 0;
+  cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(want, 1) * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return nps_fail(NPS_ERR_OOM, std::string("color workspace: cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  *have = want;
+  return NPS_OK;
+}
+
+}  // namespace
+
+extern "C" nps_status nps_color(const int32_t* row_ptr, const int32_t* col, int32_t n, int64_t m,
+                                const nps_params* pin, int32_t* color_out, nps_stats* st) {
+  nps_clear_error();
+  nps_params p;
+  if (pin) p = *pin;
+  else nps_params_default(&p);
+  if (p.threshold < 1) return nps_fail(NPS_ERR_INVALID_ARG, "threshold must be >= 1");
+  if (!(p.timeout_s > 0) || p.timeout_s > 3600) return nps_fail(NPS_ERR_INVALID_ARG, "timeout_s must be in (0, 3600]");
+  if (n <= 0) return nps_fail(NPS_ERR_INVALID_ARG, "n must be positive");
+  if (m < 0 || m >= (int64_t)INT32_MAX) return nps_fail(NPS_ERR_INVALID_ARG, "m must be in [0, 2^31-1)");
+  if (!row_ptr || !color_out || (m > 0 && !col)) return nps_fail(NPS_ERR_INVALID_ARG, "null array");
+  if (!p.device_ptrs && (row_ptr[0] != 0 || row_ptr[n] != (int32_t)m))
+    return nps_fail(NPS_ERR_FORMAT, "malformed CSR: row_ptr[0] must be 0 and row_ptr[n] must be m");
+  int dcount = 0;
+  if (cudaGetDeviceCount(&dcount) != cudaSuccess || dcount == 0) {
+    cudaGetLastError();
+    return nps_fail(NPS_ERR_NO_DEVICE, "no CUDA device");
+  }
+  if (p.device < 0 || p.device >= dcount) return nps_fail(NPS_ERR_INVALID_ARG, "device ordinal out of range");
+  CL_CUDA(cudaSetDevice(p.device));
+  ColorWork* W;
+  {
+    std::lock_guard<std::mutex> lk(g_color_mu);
+    if ((int)g_color.size() <= p.device) g_color.resize(p.device + 1, nullptr);
+    if (!g_color[p.device]) g_color[p.device] = new ColorWork();
+    W = g_color[p.device];
+  }
+  std::lock_guard<std::mutex> lk(W->mu);
+  if (!W->stream) CL_CUDA(cudaStreamCreateWithFlags(&W->stream, cudaStreamNonBlocking));
+  if (!W->ev[0]) {
+    for (auto& ev : W->ev) CL_CUDA(cudaEventCreate(&ev));
+    for (auto& ev : W->chunk_ev) CL_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  }
+  if (!W->ctr) CL_CUDA(cudaMalloc((void**)&W->ctr, sizeof(ColorCtr)));
+  if (!W->snap) CL_CUDA(cudaMallocHost((void**)&W->snap, 3 * sizeof(ColorCtr)));
+  if (!W->sms) CL_CUDA(cudaDeviceGetAttribute(&W->sms, cudaDevAttrMultiProcessorCount, p.device));
+  cudaStream_t s = p.stream ? (cudaStream_t)p.stream : W->stream;
+  if (st) memset(st, 0, sizeof(*st));
+  const auto t0 = std::chrono::steady_clock::now();
+  nps_status e;
+  CL_CUDA(cudaEventRecord(W->ev[0], s));
+  ColorArgs a;
+  a.row = row_ptr;
+  a.col = col;
+  a.color = color_out;
+  if (!p.device_ptrs) {
+    if ((e = ensure(&W->row, &W->row_n, (size_t)n + 1, s)) || (e = ensure(&W->col, &W->col_n, (size_t)m, s)) ||
+        (e = ensure(&W->color, &W->color_n, (size_t)n, s)))
+      return e;
+    CL_CUDA(cudaMemcpyAsync(W->row, row_ptr, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, s));
+    if (m > 0) CL_CUDA(cudaMemcpyAsync(W->col, col, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
+    a.row = W->row;
+    a.col = W->col;
+    a.color = W->color;
+  }
+  const int32_t nb = (int32_t)(((int64_t)n + kScanItems - 1) / kScanItems);
+  const size_t nn = (size_t)n;
+  // a round cuts at most m / kChunk + m / kHuge + 1 chunks
+  const size_t nchunks = (size_t)m / kChunk + (size_t)m / kHuge + 1;
+  if ((e = ensure(&W->buf, &W->buf_n, 4 * nn + 2 + (size_t)nb, s)) || (e = ensure(&W->rcol, &W->rcol_n, (size_t)m, s)) ||
+      (e = ensure(&W->state, &W->state_n, 2 * nn, s)) || (e = ensure(&W->chunk, &W->chunk_n, nchunks, s)))
+    return e;
+  a.n = n;
+  a.m = m;
+  a.pending = W->state;
+  a.best = W->state + nn;
+  a.chunk = W->chunk;
+  a.rrow = W->buf;  // n + 1 entries
+  a.rcur = W->buf + nn + 1;
+  a.list[0] = W->buf + 2 * nn + 1;
+  a.list[1] = W->buf + 3 * nn + 1;
+  a.bsum = W->buf + 4 * nn + 1;
+  a.rcol = W->rcol;
+  a.threshold = p.threshold;
+  a.c = W->ctr;
+  const int grid = (int)std::max<int64_t>(
+      1, std::min<int64_t>(((int64_t)n + kThreads - 1) / kThreads, (int64_t)W->sms * (2048 / kThreads)));
+  CL_CUDA(cudaMemsetAsync(W->ctr, 0, sizeof(ColorCtr), s));
+  CL_CUDA(cudaMemsetAsync(W->buf, 0, sizeof(int32_t) * (nn + 1), s));  // reverse-list counts
+  CL_CUDA(cudaMemsetAsync(W->state, 0, sizeof(int32_t) * 2 * nn, s));
+  CL_CUDA(cudaEventRecord(W->ev[1], s));
+  color_count_kernel<<<grid, kThreads, 0, s>>>(a);
+  scan_blocks_kernel<<<nb, kThreads, 0, s>>>(a.rrow, n, a.bsum);
+  scan_totals_kernel<<<1, kThreads, 0, s>>>(a.bsum, nb, a.rrow + n);
+  scan_add_kernel<<<grid, kThreads, 0, s>>>(a.rrow, n, a.bsum, a.rcur);
+  color_scatter_kernel<<<grid, kThreads, 0, s>>>(a);
+  color_first_kernel<<<grid, kThreads, 0, s>>>(a);
+  CL_CUDA(cudaGetLastError());
+  // rounds in chunks; the counters of chunk k are read while chunk k + 1 runs
+  int64_t r = 0;
+  int chunk = 4, k = 0;
+  bool done = false;
+  while (!done) {
+    for (int j = 0; j < chunk; ++j) {
+      color_round_kernel<<<grid, kThreads, 0, s>>>(a, (int)((r + j) % 3), (int)((r + j) & 1));
+      color_chunks_kernel<<<grid, kThreads, 0, s>>>(a, (int)((r + j) % 3), (int)((r + j) & 1));
+    }
+    CL_CUDA(cudaGetLastError());
+    r += chunk;
+    CL_CUDA(cudaMemcpyAsync(&W->snap[k & 1], W->ctr, sizeof(ColorCtr), cudaMemcpyDeviceToHost, s));
+    CL_CUDA(cudaEventRecord(W->chunk_ev[k & 1], s));
+    if (k > 0) {
+      CL_CUDA(cudaEventSynchronize(W->chunk_ev[(k - 1) & 1]));
+      const ColorCtr& sn = W->snap[(k - 1) & 1];
+      if (sn.status || sn.len[(r - chunk) % 3] == 0) done = true;  // the frontier of chunk k's first round
+    }
+    ++k;
+    chunk = std::min(chunk * 2, kMaxChunk);
+    if (!done && r > (int64_t)n + 2 * kMaxChunk + 8) {  // a round per color, at most n colors
+      cudaStreamSynchronize(s);
+      return nps_fail(NPS_ERR_CAPACITY, "color: did not finish within n rounds");
+    }
+    if (!done && std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > p.timeout_s) {
+      cudaStreamSynchronize(s);
+      return nps_fail(NPS_ERR_TIMEOUT, "color: exceeded timeout_s");
+    }
+  }
+  CL_CUDA(cudaEventRecord(W->ev[2], s));
+  color_left_kernel<<<grid, kThreads, 0, s>>>(a.color, n, &W->ctr->left);
+  CL_CUDA(cudaGetLastError());
+  if (!p.device_ptrs)
+    CL_CUDA(cudaMemcpyAsync(color_out, a.color, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost, s));
+  CL_CUDA(cudaMemcpyAsync(&W->snap[2], W->ctr, sizeof(ColorCtr), cudaMemcpyDeviceToHost, s));
+  CL_CUDA(cudaEventRecord(W->ev[3], s));
+  CL_CUDA(cudaStreamSynchronize(s));
+  const ColorCtr& f = W->snap[2];
+  if (st) {
+    st->status = (int32_t)f.status;
+    st->iterations = (uint32_t)f.max_color;  // the reference's iteration count: one color per iteration
+    st->buckets = f.rounds;                  // rounds here (one per color after the first)
+    st->edges_scanned = f.edges;
+    st->grid_ctas = grid;
+    cudaEventElapsedTime(&st->kernel_ms, W->ev[1], W->ev[2]);
+    cudaEventElapsedTime(&st->total_ms, W->ev[0], W->ev[3]);
+  }
+  if (f.status == NPS_ERR_FORMAT)
+    return nps_fail(NPS_ERR_FORMAT, "malformed CSR: a row range or column index is out of bounds");
+  if (f.left) return nps_fail(NPS_ERR_CAPACITY, "color: " + std::to_string(f.left) + " vertices left uncolored");
+  return NPS_OK;
+}

@@ -54,6 +54,10 @@ def _load_oracle():
         lib.oracle_fnv1a_u32.restype = C.c_uint64
         lib.oracle_bc.argtypes = [_I32, _P, _P, _I32, _P, _P]
         lib.oracle_bc.restype = C.c_int
+        lib.oracle_color.argtypes = [_I32, _P, _P, _P]
+        lib.oracle_color.restype = _I32
+        lib.oracle_color_iterations.argtypes = [_I32, _P, _P, _P]
+        lib.oracle_color_iterations.restype = _I32
         _orc = lib
     return _orc
 
@@ -291,6 +295,20 @@ def bc(row, col, sources=None):
     if rc != 0:
         raise RuntimeError("oracle_bc: out of memory")
     return out
+
+
+def color(row, col, literal=False):
+    """The graph-color application's colors (gclr_bitmap_kernel,
+    apps/graph-color/src/gpu/graph_color_kernel.cu:14-35): (int32 colors, the
+    iteration count).  literal=True simulates the reference's iterations one by
+    one (O(n x iterations)); the default is the closed form in id order."""
+    row = np.ascontiguousarray(row, dtype=np.int32)
+    col = np.ascontiguousarray(col, dtype=np.int32)
+    n = row.shape[0] - 1
+    out = np.zeros(n, dtype=np.int32)
+    fn = _load_oracle().oracle_color_iterations if literal else _load_oracle().oracle_color
+    it = fn(n, row.ctypes.data, col.ctypes.data, out.ctypes.data)
+    return out, int(it)
 
 
 def have_reference_bc() -> bool:

@@ -37,6 +37,15 @@
  *                      reached v other than the source (:83-101).  MAX_LEVEL = 9999
  *                      marks unvisited vertices, as in common/global.h:17.
  *
+ *   oracle_color       the coloring of the graph-color application
+ *                      (gclr_bitmap_kernel, apps/graph-color/src/gpu/graph_color_kernel.cu:14-35,
+ *                      iterated by gclr_nopruning_gpu, graph_color_wrapper.cu:113-130): in iteration c an
+ *                      uncolored v takes c unless an out-neighbour u < v is uncolored
+ *                      or colored c.  Both block v whatever the order, so v ends with
+ *                      1 + the largest color of its smaller out-neighbours; in id order
+ *                      those are final when v is reached.  The reference has no CPU
+ *                      version of this path (parity unpinned: see the test header).
+ *
  * Distances are uint32 with INF = 2^30 (sssp_wrapper.cu:7, common/global.h:19).
  * A tentative distance that reaches 2^30 is treated as unreachable; the
  * reference's int arithmetic never gets there on the inputs it is run on.
@@ -355,4 +364,45 @@ int oracle_bc(int32_t n, const int32_t* row, const int32_t* col, int32_t nsrc, c
   }
   free(level), free(sigma), free(delta), free(order), free(lb);
   return 0;
+}
+
+/* Colors of the graph-color application's iterations (see the header); returns
+ * the iteration count, the largest color. */
+int32_t oracle_color(int32_t n, const int32_t* row, const int32_t* col, int32_t* color) {
+  int32_t most = 0;
+  for (int32_t v = 0; v < n; ++v) {
+    int32_t c = 0;
+    for (int32_t e = row[v]; e < row[v + 1]; ++e) {
+      const int32_t u = col[e];
+      if (u < v && color[u] > c) c = color[u];
+    }
+    color[v] = c + 1;
+    if (c + 1 > most) most = c + 1;
+  }
+  return most;
+}
+
+/* The same by simulating the reference's iterations literally: every iteration
+ * tests every uncolored vertex against the colors at that moment (vertices in id
+ * order, so a vertex colored earlier in the iteration is seen with color c, as a
+ * racing GPU thread may see it).  Returns the iteration count. */
+int32_t oracle_color_iterations(int32_t n, const int32_t* row, const int32_t* col, int32_t* color) {
+  for (int32_t v = 0; v < n; ++v) color[v] = 0;
+  int32_t c = 0, left = n;
+  while (left > 0) {
+    ++c;
+    for (int32_t v = 0; v < n; ++v) {
+      if (color[v] != 0) continue;
+      int ok = 1;
+      for (int32_t e = row[v]; e < row[v + 1] && ok; ++e) {
+        const int32_t u = col[e];
+        if ((color[u] == 0 || color[u] == c) && u < v) ok = 0;
+      }
+      if (ok) {
+        color[v] = c;
+        --left;
+      }
+    }
+  }
+  return c;
 }
