@@ -26,14 +26,13 @@
 // dependency counts are built, shorter ones by one thread.  In a round, a warp
 // walks the reverse lists of 32 frontier vertices flat, 32 entries per step, and
 // reverse lists of kHuge entries or more (the hubs: vertex 0 of an R-MAT graph
-// has millions of dependants) are cut into chunks that a second kernel of the
-// round spreads over every warp -- the warp / grid consolidation of long rows.  Rounds are
-// enqueued in chunks and the host reads the frontier length once per chunk, as
-// for the SSSP solutions 0-5.
+// has millions of dependants) are cut into chunks that the round's second pass
+// spreads over every warp -- the warp / grid consolidation of long rows.  All
+// rounds run in one persistent cooperative launch with a bounded grid barrier
+// between passes, instead of a launch and a host round trip per iteration.
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <chrono>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -46,7 +45,6 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kScanItems = 1024;  // elements per CTA of the scan (4 per thread)
-constexpr int kMaxChunk = 32;      // rounds per host read-back, at most
 constexpr int32_t kHuge = 256;     // reverse lists this long are cut into chunks for all warps
 constexpr int32_t kChunk = 256;    // entries per chunk
 constexpr unsigned kFull = 0xffffffffu;
@@ -226,20 +224,47 @@ __device__ __forceinline__ int32_t settle(const ColorArgs& a, int32_t w, int32_t
   return cw;
 }
 
-// Round r (r3 = r % 3, par = r & 1): walk the reverse lists of frontier list[par].
-// A warp takes 32 frontier vertices and walks their reverse lists flat, 32
-// entries per step (a 5-step shuffle search finds each entry's vertex), so the
-// longest chain of dependent atomics in a warp is its lists' total / 32.  Lists
-// of kHuge entries or more are cut into kChunk pieces for color_chunks_kernel,
-// which runs next and spreads them over every warp.
-__global__ void __launch_bounds__(kThreads) color_round_kernel(ColorArgs a, int r3, int par) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    a.c->len[(r3 + 2) % 3] = 0;
-    a.c->chunks[(r3 + 2) % 3] = 0;
+// settle() for up to kBatch dependants of one lane at once: the maxima are
+// issued together, one fence orders them before the decrements, the decrements
+// are issued together, and one more fence precedes the reads of best by the
+// lanes whose decrement reached 0 -- two round trips per batch instead of two
+// per dependant.
+constexpr int kBatch = 4;
+__device__ __forceinline__ int32_t settle_batch(const ColorArgs& a, const int32_t (&w)[kBatch],
+                                                const int32_t (&cv)[kBatch], const bool (&ok)[kBatch], int32_t* out,
+                                                uint32_t* len) {
+#pragma unroll
+  for (int j = 0; j < kBatch; ++j)
+    if (ok[j]) atomicMax(a.best + w[j], cv[j]);
+  __threadfence();
+  int32_t left[kBatch];
+#pragma unroll
+  for (int j = 0; j < kBatch; ++j) left[j] = ok[j] ? atomicSub(a.pending + w[j], 1) : 0;
+  int32_t most = 0;
+  bool any = false;
+#pragma unroll
+  for (int j = 0; j < kBatch; ++j) any |= left[j] == 1;
+  if (any) {
+    __threadfence();
+#pragma unroll
+    for (int j = 0; j < kBatch; ++j) {
+      if (left[j] != 1) continue;
+      const int32_t cw = __ldcg(a.best + w[j]) + 1;
+      a.color[w[j]] = cw;
+      out[atomicAdd(len, 1u)] = w[j];
+      most = max(most, cw);
+    }
   }
-  const uint32_t len = a.c->len[r3];
-  if (len == 0) return;
-  if (blockIdx.x == 0 && threadIdx.x == 0) a.c->rounds += 1;
+  return most;
+}
+
+// Round r (r3 = r % 3, par = r & 1), first pass: walk the reverse lists of the
+// len vertices of frontier list[par].  A warp takes 32 frontier vertices and
+// walks their reverse lists flat, 32 entries per step (a 5-step shuffle search
+// finds each entry's vertex), so the longest chain of dependent atomics in a
+// warp is its lists' total / 32.  Lists of kHuge entries or more are cut into
+// kChunk pieces for the second pass, which spreads them over every warp.
+__device__ __forceinline__ void round_walk(const ColorArgs& a, int r3, int par, uint32_t len) {
   const int lane = threadIdx.x & 31;
   const int32_t* in = a.list[par];
   int32_t* out = a.list[par ^ 1];
@@ -267,17 +292,25 @@ __global__ void __launch_bounds__(kThreads) color_round_kernel(ColorArgs a, int 
       if (lane >= o) incl += t;
     }
     const uint32_t excl = incl - flat, total = __shfl_sync(kFull, incl, 31);
-    for (uint32_t fb = 0; fb < total; fb += 32) {
-      const uint32_t k = fb + lane;
-      int o = 0;  // the last lane whose prefix is <= k
+    for (uint32_t fb = 0; fb < total; fb += 32 * kBatch) {  // kBatch entries per lane per step
+      int32_t w[kBatch], c[kBatch];
+      bool ok[kBatch];
 #pragma unroll
-      for (int step = 16; step >= 1; step >>= 1) {
-        const uint32_t x = __shfl_sync(kFull, excl, o + step);
-        if (x <= k) o += step;
+      for (int j = 0; j < kBatch; ++j) {
+        const uint32_t k = fb + 32 * j + lane;
+        int o = 0;  // the last lane whose prefix is <= k
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1) {
+          const uint32_t x = __shfl_sync(kFull, excl, o + step);
+          if (x <= k) o += step;
+        }
+        const int32_t os = __shfl_sync(kFull, s, o), oc = __shfl_sync(kFull, cv, o);
+        const uint32_t oe = __shfl_sync(kFull, excl, o);
+        ok[j] = k < total;
+        w[j] = ok[j] ? a.rcol[os + (int32_t)(k - oe)] : 0;
+        c[j] = oc;
       }
-      const int32_t os = __shfl_sync(kFull, s, o), oc = __shfl_sync(kFull, cv, o);
-      const uint32_t oe = __shfl_sync(kFull, excl, o);
-      if (k < total) most = max(most, settle(a, a.rcol[os + (int32_t)(k - oe)], oc, out, out_len));
+      most = max(most, settle_batch(a, w, c, ok, out, out_len));
     }
     // huge lists: one chunk descriptor per kChunk entries, reserved once per warp
     const uint32_t nch = huge ? (uint32_t)((d + kChunk - 1) / kChunk) : 0u;
@@ -306,10 +339,9 @@ __global__ void __launch_bounds__(kThreads) color_round_kernel(ColorArgs a, int 
   }
 }
 
-// The same round, second pass: one warp per chunk of a huge reverse list.
-__global__ void __launch_bounds__(kThreads) color_chunks_kernel(ColorArgs a, int r3, int par) {
-  const uint32_t nc = a.c->chunks[r3];
-  if (nc == 0) return;
+// The same round, second pass: one warp per chunk of the nc chunks of huge
+// reverse lists.
+__device__ __forceinline__ void round_chunks(const ColorArgs& a, int r3, int par, uint32_t nc) {
   const int lane = threadIdx.x & 31;
   int32_t* out = a.list[par ^ 1];
   uint32_t* out_len = &a.c->len[(r3 + 1) % 3];
@@ -317,10 +349,92 @@ __global__ void __launch_bounds__(kThreads) color_chunks_kernel(ColorArgs a, int
   const uint32_t warps = gridDim.x * (kThreads / 32);
   for (uint32_t q = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5); q < nc; q += warps) {
     const int4 cd = a.chunk[q];  // {vertex, first, end, its color}
-    for (int32_t k = cd.y + lane; k < cd.z; k += 32) most = max(most, settle(a, a.rcol[k], cd.w, out, out_len));
+    for (int32_t k0 = cd.y + lane; k0 < cd.z; k0 += 32 * kBatch) {
+      int32_t w[kBatch], c[kBatch];
+      bool ok[kBatch];
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) {
+        const int32_t k = k0 + 32 * j;
+        ok[j] = k < cd.z;
+        w[j] = ok[j] ? a.rcol[k] : 0;
+        c[j] = cd.w;
+      }
+      most = max(most, settle_batch(a, w, c, ok, out, out_len));
+    }
   }
   most = __reduce_max_sync(kFull, most);
   if (lane == 0 && most) atomicMax(&a.c->max_color, most);
+}
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ uint32_t ld_volatile_u32(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.volatile.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid-wide barrier of the persistent kernel: one arrival per CTA on a
+// monotonic counter, then a wait for epoch x CTAs arrivals.  The wait is bounded
+// by timeout_ns (then the status becomes NPS_ERR_TIMEOUT and the abort word is
+// set) and ends early when another CTA aborted.  Returns false on either.
+__device__ bool grid_barrier(uint32_t* bar, uint32_t& epoch, uint32_t ctas, uint32_t* abort_word, uint32_t* status,
+                             unsigned long long timeout_ns) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    epoch += 1;
+    __threadfence();  // this CTA's writes before its arrival
+    atomicAdd(bar, 1u);
+    const uint32_t target = epoch * ctas;
+    const unsigned long long t0 = globaltimer_ns();
+    int ok = 1;
+    while ((int32_t)(ld_volatile_u32(bar) - target) < 0) {
+      if (ld_volatile_u32(abort_word)) {
+        ok = 0;
+        break;
+      }
+      if (globaltimer_ns() - t0 > timeout_ns) {
+        atomicCAS(status, 0u, (uint32_t)NPS_ERR_TIMEOUT);
+        atomicExch(abort_word, 1u);
+        ok = 0;
+        break;
+      }
+      __nanosleep(32);
+    }
+    __threadfence();  // every arrival's writes before what follows
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Every round in one cooperative launch (all CTAs resident), two grid barriers
+// per round: first pass, barrier, second pass, barrier.  The frontier and chunk
+// counts are read after a barrier, so every CTA sees the same ones and leaves
+// the loop together.
+__global__ void __launch_bounds__(kThreads) color_rounds_kernel(ColorArgs a, uint32_t* bar, uint32_t* abort_word,
+                                                                unsigned long long timeout_ns) {
+  uint32_t epoch = 0;
+  for (uint32_t r = 0;; ++r) {
+    const int r3 = (int)(r % 3), par = (int)(r & 1);
+    const uint32_t len = __ldcg(&a.c->len[r3]);
+    if (len == 0) break;  // a malformed entry is skipped, not a reason to stop: every CTA stops together
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      a.c->len[(r3 + 2) % 3] = 0;  // read in round r - 1, filled in round r + 1
+      a.c->chunks[(r3 + 2) % 3] = 0;
+      a.c->rounds += 1;
+    }
+    round_walk(a, r3, par, len);
+    if (!grid_barrier(bar, epoch, gridDim.x, abort_word, &a.c->status, timeout_ns)) return;
+    const uint32_t nc = __ldcg(&a.c->chunks[r3]);
+    if (nc) round_chunks(a, r3, par, nc);
+    if (!grid_barrier(bar, epoch, gridDim.x, abort_word, &a.c->status, timeout_ns)) return;
+  }
 }
 
 __global__ void color_left_kernel(const int32_t* color, int32_t n, uint32_t* left) {
@@ -342,10 +456,10 @@ struct ColorWork {
   std::mutex mu;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[4] = {};
-  cudaEvent_t chunk_ev[2] = {};
   int sms = 0;
   ColorCtr* ctr = nullptr;
-  ColorCtr* snap = nullptr;  // pinned: [0], [1] per chunk, [2] final
+  ColorCtr* snap = nullptr;  // pinned: [2] final
+  uint32_t* bar = nullptr;   // grid barrier counter and abort word
   int32_t* buf = nullptr;    // rrow, rcur, list 0, list 1, scan totals
   size_t buf_n = 0;
   int32_t* state = nullptr;  // pending, best
@@ -417,14 +531,13 @@ extern "C" nps_status nps_color(const int32_t* row_ptr, const int32_t* col, int3
   if (!W->stream) CL_CUDA(cudaStreamCreateWithFlags(&W->stream, cudaStreamNonBlocking));
   if (!W->ev[0]) {
     for (auto& ev : W->ev) CL_CUDA(cudaEventCreate(&ev));
-    for (auto& ev : W->chunk_ev) CL_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   }
   if (!W->ctr) CL_CUDA(cudaMalloc((void**)&W->ctr, sizeof(ColorCtr)));
   if (!W->snap) CL_CUDA(cudaMallocHost((void**)&W->snap, 3 * sizeof(ColorCtr)));
+  if (!W->bar) CL_CUDA(cudaMalloc((void**)&W->bar, 2 * sizeof(uint32_t)));
   if (!W->sms) CL_CUDA(cudaDeviceGetAttribute(&W->sms, cudaDevAttrMultiProcessorCount, p.device));
   cudaStream_t s = p.stream ? (cudaStream_t)p.stream : W->stream;
   if (st) memset(st, 0, sizeof(*st));
-  const auto t0 = std::chrono::steady_clock::now();
   nps_status e;
   CL_CUDA(cudaEventRecord(W->ev[0], s));
   ColorArgs a;
@@ -474,34 +587,17 @@ extern "C" nps_status nps_color(const int32_t* row_ptr, const int32_t* col, int3
   color_scatter_kernel<<<grid, kThreads, 0, s>>>(a);
   color_first_kernel<<<grid, kThreads, 0, s>>>(a);
   CL_CUDA(cudaGetLastError());
-  // rounds in chunks; the counters of chunk k are read while chunk k + 1 runs
-  int64_t r = 0;
-  int chunk = 4, k = 0;
-  bool done = false;
-  while (!done) {
-    for (int j = 0; j < chunk; ++j) {
-      color_round_kernel<<<grid, kThreads, 0, s>>>(a, (int)((r + j) % 3), (int)((r + j) & 1));
-      color_chunks_kernel<<<grid, kThreads, 0, s>>>(a, (int)((r + j) % 3), (int)((r + j) & 1));
-    }
-    CL_CUDA(cudaGetLastError());
-    r += chunk;
-    CL_CUDA(cudaMemcpyAsync(&W->snap[k & 1], W->ctr, sizeof(ColorCtr), cudaMemcpyDeviceToHost, s));
-    CL_CUDA(cudaEventRecord(W->chunk_ev[k & 1], s));
-    if (k > 0) {
-      CL_CUDA(cudaEventSynchronize(W->chunk_ev[(k - 1) & 1]));
-      const ColorCtr& sn = W->snap[(k - 1) & 1];
-      if (sn.status || sn.len[(r - chunk) % 3] == 0) done = true;  // the frontier of chunk k's first round
-    }
-    ++k;
-    chunk = std::min(chunk * 2, kMaxChunk);
-    if (!done && r > (int64_t)n + 2 * kMaxChunk + 8) {  // a round per color, at most n colors
-      cudaStreamSynchronize(s);
-      return nps_fail(NPS_ERR_CAPACITY, "color: did not finish within n rounds");
-    }
-    if (!done && std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > p.timeout_s) {
-      cudaStreamSynchronize(s);
-      return nps_fail(NPS_ERR_TIMEOUT, "color: exceeded timeout_s");
-    }
+  // every round in one cooperative launch, as many CTAs as are resident
+  int per_sm = 0;
+  CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, color_rounds_kernel, kThreads, 0));
+  const int rgrid = std::max(1, std::min(W->sms * std::max(1, per_sm), grid));
+  CL_CUDA(cudaMemsetAsync(W->bar, 0, 2 * sizeof(uint32_t), s));
+  {
+    uint32_t* bar = W->bar;
+    uint32_t* abort_word = W->bar + 1;
+    unsigned long long timeout_ns = (unsigned long long)(p.timeout_s * 1e9);
+    void* args[] = {&a, &bar, &abort_word, &timeout_ns};
+    CL_CUDA(cudaLaunchCooperativeKernel((const void*)color_rounds_kernel, dim3(rgrid), dim3(kThreads), args, 0, s));
   }
   CL_CUDA(cudaEventRecord(W->ev[2], s));
   color_left_kernel<<<grid, kThreads, 0, s>>>(a.color, n, &W->ctr->left);
@@ -523,6 +619,7 @@ extern "C" nps_status nps_color(const int32_t* row_ptr, const int32_t* col, int3
   }
   if (f.status == NPS_ERR_FORMAT)
     return nps_fail(NPS_ERR_FORMAT, "malformed CSR: a row range or column index is out of bounds");
+  if (f.status == NPS_ERR_TIMEOUT) return nps_fail(NPS_ERR_TIMEOUT, "color: a grid barrier wait exceeded timeout_s");
   if (f.left) return nps_fail(NPS_ERR_CAPACITY, "color: " + std::to_string(f.left) + " vertices left uncolored");
   return NPS_OK;
 }
