@@ -101,6 +101,16 @@ def make_graph(nps, name):
     return nps.gen_uniform(a["n"], a["m"], a["wmax"], a["seed"])
 
 
+def _traffic(key):
+    """DRAM bytes of one launch of the workload's dominant kernel, from the ncu capture recorded
+    in profiles/traffic.json (null when none was recorded)."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        return json.load(f).get(key)
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -684,7 +694,7 @@ def bench_bfs(a, nps, ws, rank, local, desc):
                                   "iterations": lv_st.iterations, "buckets": lv_st.buckets,
                                   "exact_vs_oracle": lv_exact},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "peak_source": peak_src, "b_alg_bytes": b_alg,
+                         "traffic": _traffic("bfs22"), "peak_source": peak_src, "b_alg_bytes": b_alg,
                          "b_alg_formula": "8*m_r + 12*n_r + 4*n"},
             "e2e": {"value": ws * m_r / (e2e_ms * 1e-3) / 1e9, "unit": "GTEPS", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": 4 * (g.n + 1) + 4 * g.m, "d2h_bytes_per_step": 4 * g.n,

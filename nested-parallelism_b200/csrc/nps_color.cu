@@ -45,8 +45,12 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kScanItems = 1024;  // elements per CTA of the scan (4 per thread)
-constexpr int32_t kHuge = 256;     // reverse lists this long are cut into chunks for all warps
-constexpr int32_t kChunk = 256;    // entries per chunk
+// Measured on R-MAT scale 22 (1,295 rounds): (kHuge, kChunk) = (256, 256) 69 ms,
+// (64, 256) 55 ms, (32, 128) 43 ms -- shorter flat walks per warp shorten each
+// round's slowest chain; 1, 2 or 4 CTAs per SM made no difference.
+constexpr int kRoundCtasPerSm = 2;  // CTAs per SM of the persistent round kernel by default
+constexpr int32_t kHuge = 32;       // reverse lists this long are cut into chunks for all warps
+constexpr int32_t kChunk = 128;     // entries per chunk (one step of a warp: 4 per lane)
 constexpr unsigned kFull = 0xffffffffu;
 
 struct ColorCtr {
@@ -260,9 +264,9 @@ __device__ __forceinline__ int32_t settle_batch(const ColorArgs& a, const int32_
 
 // Round r (r3 = r % 3, par = r & 1), first pass: walk the reverse lists of the
 // len vertices of frontier list[par].  A warp takes 32 frontier vertices and
-// walks their reverse lists flat, 32 entries per step (a 5-step shuffle search
+// walks their reverse lists flat, 128 entries per step (a 5-step shuffle search
 // finds each entry's vertex), so the longest chain of dependent atomics in a
-// warp is its lists' total / 32.  Lists of kHuge entries or more are cut into
+// warp is its lists' total / 128.  Lists of kHuge entries or more are cut into
 // kChunk pieces for the second pass, which spreads them over every warp.
 __device__ __forceinline__ void round_walk(const ColorArgs& a, int r3, int par, uint32_t len) {
   const int lane = threadIdx.x & 31;
@@ -388,8 +392,8 @@ __device__ bool grid_barrier(uint32_t* bar, uint32_t& epoch, uint32_t ctas, uint
   __syncthreads();
   if (threadIdx.x == 0) {
     epoch += 1;
-    __threadfence();  // this CTA's writes before its arrival
-    atomicAdd(bar, 1u);
+    // the arrival releases this CTA's writes (ordered after the barrier above)
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
     const uint32_t target = epoch * ctas;
     const unsigned long long t0 = globaltimer_ns();
     int ok = 1;
@@ -406,7 +410,11 @@ __device__ bool grid_barrier(uint32_t* bar, uint32_t& epoch, uint32_t ctas, uint
       }
       __nanosleep(32);
     }
-    __threadfence();  // every arrival's writes before what follows
+    if (ok) {  // acquire: every arrival's writes before what follows
+      uint32_t v;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+      (void)v;
+    }
     s_ok = ok;
   }
   __syncthreads();
@@ -590,7 +598,9 @@ extern "C" nps_status nps_color(const int32_t* row_ptr, const int32_t* col, int3
   // every round in one cooperative launch, as many CTAs as are resident
   int per_sm = 0;
   CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, color_rounds_kernel, kThreads, 0));
-  const int rgrid = std::max(1, std::min(W->sms * std::max(1, per_sm), grid));
+  // p.ctas_per_sm picks fewer CTAs (cheaper barriers) than the resident maximum
+  const int use = p.ctas_per_sm > 0 ? std::min(p.ctas_per_sm, std::max(1, per_sm)) : kRoundCtasPerSm;
+  const int rgrid = std::max(1, std::min(W->sms * std::min(use, std::max(1, per_sm)), grid));
   CL_CUDA(cudaMemsetAsync(W->bar, 0, 2 * sizeof(uint32_t), s));
   {
     uint32_t* bar = W->bar;
