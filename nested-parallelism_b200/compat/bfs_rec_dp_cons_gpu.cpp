@@ -34,6 +34,8 @@ void bfs_rec_dp_cons_gpu() {
   nps_params_default(&p);
   p.level = CONSOLIDATE_LEVEL;
   p.delta = 0;
+  p.threshold = 32;     // the tuned BFS configuration (nps.bfs_params)
+  p.block_size = 512;
   p.device_ptrs = 1;
   nps_stats st;
   nps_compat_bfs_last_status = nps_bfs(reinterpret_cast<const int32_t*>(d_vertexArray),
