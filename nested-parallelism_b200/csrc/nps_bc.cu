@@ -331,8 +331,11 @@ extern "C" nps_status nps_bc(const int32_t* row_ptr, const int32_t* col, int32_t
   // sources shares one delta buffer
   int per_sm = 0;
   BC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bc_sources_kernel, kThreads, 0));
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)W->sms * std::max(1, per_sm), count_all));
   const size_t per_cta = 4 * (size_t)n + 2;
+  // at most 8 GB of CTA scratch (16 n bytes each): large graphs run fewer sources at once
+  const int64_t by_memory = std::max<int64_t>(W->sms, (int64_t)((8ull << 30) / (per_cta * sizeof(int32_t))));
+  const int grid = (int)std::max<int64_t>(
+      1, std::min<int64_t>(std::min<int64_t>((int64_t)W->sms * std::max(1, per_sm), by_memory), count_all));
   if ((e = ensure(&W->scratch, &W->scratch_n, per_cta * (size_t)grid, s))) return e;
   const size_t budget = (size_t)1 << 31;  // bytes of delta rows per block
   int64_t cap = std::max<int64_t>(grid, budget / (4 * (size_t)n));
