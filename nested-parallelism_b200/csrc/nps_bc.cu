@@ -216,12 +216,6 @@ __global__ void bc_check_sources_kernel(const int32_t* sources, int32_t nsrc, in
     if ((uint32_t)sources[i] >= (uint32_t)n) atomicCAS(status, 0u, (uint32_t)NPS_ERR_INVALID_ARG);
 }
 
-#define BC_CUDA(call)                                                                         \
-  do {                                                                                        \
-    cudaError_t e_ = (call);                                                                  \
-    if (e_ != cudaSuccess)                                                                    \
-      return nps_fail(NPS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
-  } while (0)
 
 struct BcWork {
   std::mutex mu;
@@ -246,24 +240,6 @@ struct BcWork {
 std::mutex g_bc_mu;
 std::vector<BcWork*> g_bc;
 
-template <class T>
-nps_status ensure(T** p, size_t* have, size_t want, cudaStream_t s) {
-  if (*p && *have >= want) return NPS_OK;
-  if (*p) {
-    cudaStreamSynchronize(s);
-    cudaFree(*p);
-  }
-  *p = nullptr;
-  *have = 0;
-  cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(want, 1) * sizeof(T));
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    *p = nullptr;
-    return nps_fail(NPS_ERR_OOM, std::string("bc workspace: cudaMalloc: ") + cudaGetErrorString(e));
-  }
-  *have = want;
-  return NPS_OK;
-}
 
 }  // namespace
 
@@ -290,7 +266,7 @@ extern "C" nps_status nps_bc(const int32_t* row_ptr, const int32_t* col, int32_t
     return nps_fail(NPS_ERR_NO_DEVICE, "no CUDA device");
   }
   if (p.device < 0 || p.device >= dcount) return nps_fail(NPS_ERR_INVALID_ARG, "device ordinal out of range");
-  BC_CUDA(cudaSetDevice(p.device));
+  NPS_CUDA_RETURN(cudaSetDevice(p.device));
   BcWork* W;
   {
     std::lock_guard<std::mutex> lk(g_bc_mu);
@@ -299,28 +275,28 @@ extern "C" nps_status nps_bc(const int32_t* row_ptr, const int32_t* col, int32_t
     W = g_bc[p.device];
   }
   std::lock_guard<std::mutex> lk(W->mu);
-  if (!W->stream) BC_CUDA(cudaStreamCreateWithFlags(&W->stream, cudaStreamNonBlocking));
+  if (!W->stream) NPS_CUDA_RETURN(cudaStreamCreateWithFlags(&W->stream, cudaStreamNonBlocking));
   if (!W->ev[0])
-    for (auto& ev : W->ev) BC_CUDA(cudaEventCreate(&ev));
-  if (!W->status) BC_CUDA(cudaMalloc((void**)&W->status, sizeof(uint32_t)));
-  if (!W->sms) BC_CUDA(cudaDeviceGetAttribute(&W->sms, cudaDevAttrMultiProcessorCount, p.device));
+    for (auto& ev : W->ev) NPS_CUDA_RETURN(cudaEventCreate(&ev));
+  if (!W->status) NPS_CUDA_RETURN(cudaMalloc((void**)&W->status, sizeof(uint32_t)));
+  if (!W->sms) NPS_CUDA_RETURN(cudaDeviceGetAttribute(&W->sms, cudaDevAttrMultiProcessorCount, p.device));
   cudaStream_t s = p.stream ? (cudaStream_t)p.stream : W->stream;
   if (st) memset(st, 0, sizeof(*st));
   nps_status e;
-  BC_CUDA(cudaEventRecord(W->ev[0], s));
+  NPS_CUDA_RETURN(cudaEventRecord(W->ev[0], s));
   const int32_t* drow = row_ptr;
   const int32_t* dcol = col;
   const int32_t* dsrc = sources;
   float* dbc = bc_out;
   if (!p.device_ptrs) {
-    if ((e = ensure(&W->row, &W->row_n, (size_t)n + 1, s)) || (e = ensure(&W->col, &W->col_n, (size_t)m, s)) ||
-        (e = ensure(&W->bc, &W->bc_n, (size_t)n, s)))
+    if ((e = nps_ensure(&W->row, &W->row_n, (size_t)n + 1, s, "bc")) || (e = nps_ensure(&W->col, &W->col_n, (size_t)m, s, "bc")) ||
+        (e = nps_ensure(&W->bc, &W->bc_n, (size_t)n, s, "bc")))
       return e;
-    BC_CUDA(cudaMemcpyAsync(W->row, row_ptr, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, s));
-    if (m > 0) BC_CUDA(cudaMemcpyAsync(W->col, col, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
+    NPS_CUDA_RETURN(cudaMemcpyAsync(W->row, row_ptr, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, s));
+    if (m > 0) NPS_CUDA_RETURN(cudaMemcpyAsync(W->col, col, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
     if (sources && nsrc > 0) {
-      if ((e = ensure(&W->src, &W->src_n, (size_t)nsrc, s))) return e;
-      BC_CUDA(cudaMemcpyAsync(W->src, sources, sizeof(int32_t) * (size_t)nsrc, cudaMemcpyHostToDevice, s));
+      if ((e = nps_ensure(&W->src, &W->src_n, (size_t)nsrc, s, "bc"))) return e;
+      NPS_CUDA_RETURN(cudaMemcpyAsync(W->src, sources, sizeof(int32_t) * (size_t)nsrc, cudaMemcpyHostToDevice, s));
       dsrc = W->src;
     }
     drow = W->row;
@@ -330,23 +306,23 @@ extern "C" nps_status nps_bc(const int32_t* row_ptr, const int32_t* col, int32_t
   // one CTA per source at a time, as many CTAs as are resident; a block of
   // sources shares one delta buffer
   int per_sm = 0;
-  BC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bc_sources_kernel, kThreads, 0));
+  NPS_CUDA_RETURN(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bc_sources_kernel, kThreads, 0));
   const size_t per_cta = 4 * (size_t)n + 2;
   // at most 8 GB of CTA scratch (16 n bytes each): large graphs run fewer sources at once
   const int64_t by_memory = std::max<int64_t>(W->sms, (int64_t)((8ull << 30) / (per_cta * sizeof(int32_t))));
   const int grid = (int)std::max<int64_t>(
       1, std::min<int64_t>(std::min<int64_t>((int64_t)W->sms * std::max(1, per_sm), by_memory), count_all));
-  if ((e = ensure(&W->scratch, &W->scratch_n, per_cta * (size_t)grid, s))) return e;
+  if ((e = nps_ensure(&W->scratch, &W->scratch_n, per_cta * (size_t)grid, s, "bc"))) return e;
   const size_t budget = (size_t)1 << 31;  // bytes of delta rows per block
   int64_t cap = std::max<int64_t>(grid, budget / (4 * (size_t)n));
   if (p.reserved[1] > 0) cap = p.reserved[1];
   const int32_t block = (int32_t)std::max<int64_t>(1, std::min<int64_t>(count_all, cap));
-  if ((e = ensure(&W->delta, &W->delta_n, (size_t)block * (size_t)n, s))) return e;
-  BC_CUDA(cudaMemsetAsync(W->status, 0, sizeof(uint32_t), s));
-  BC_CUDA(cudaMemsetAsync(dbc, 0, sizeof(float) * (size_t)n, s));
+  if ((e = nps_ensure(&W->delta, &W->delta_n, (size_t)block * (size_t)n, s, "bc"))) return e;
+  NPS_CUDA_RETURN(cudaMemsetAsync(W->status, 0, sizeof(uint32_t), s));
+  NPS_CUDA_RETURN(cudaMemsetAsync(dbc, 0, sizeof(float) * (size_t)n, s));
   if (dsrc && nsrc > 0 && p.device_ptrs) {
     bc_check_sources_kernel<<<std::min(1024, (nsrc + 255) / 256), 256, 0, s>>>(dsrc, nsrc, n, W->status);
-    BC_CUDA(cudaGetLastError());
+    NPS_CUDA_RETURN(cudaGetLastError());
   }
   BcArgs a;
   a.row = drow;
@@ -361,28 +337,28 @@ extern "C" nps_status nps_bc(const int32_t* row_ptr, const int32_t* col, int32_t
   a.delta = W->delta;
   a.status = W->status;
   bc_fill_kernel<<<W->sms * 4, 256, 0, s>>>(a.level, a.sigma, (size_t)n * grid);
-  BC_CUDA(cudaGetLastError());
+  NPS_CUDA_RETURN(cudaGetLastError());
   uint32_t h_status = 0;
   if (dsrc && p.device_ptrs) {  // a bad device-side source list stops the call before any kernel reads it
-    BC_CUDA(cudaMemcpyAsync(&h_status, W->status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    BC_CUDA(cudaStreamSynchronize(s));
+    NPS_CUDA_RETURN(cudaMemcpyAsync(&h_status, W->status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    NPS_CUDA_RETURN(cudaStreamSynchronize(s));
     if (h_status) return nps_fail(NPS_ERR_INVALID_ARG, "bc: source out of range");
   }
-  BC_CUDA(cudaEventRecord(W->ev[1], s));
+  NPS_CUDA_RETURN(cudaEventRecord(W->ev[1], s));
   const int fold_grid = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)n + 255) / 256, (int64_t)W->sms * 8));
   for (int32_t base = 0; base < count_all; base += block) {
     a.src_base = base;
     a.count = std::min<int32_t>(block, count_all - base);
     bc_sources_kernel<<<grid, kThreads, 0, s>>>(a);
-    BC_CUDA(cudaGetLastError());
+    NPS_CUDA_RETURN(cudaGetLastError());
     bc_fold_kernel<<<fold_grid, 256, 0, s>>>(dbc, W->delta, n, a.count);
-    BC_CUDA(cudaGetLastError());
+    NPS_CUDA_RETURN(cudaGetLastError());
   }
-  BC_CUDA(cudaEventRecord(W->ev[2], s));
-  if (!p.device_ptrs) BC_CUDA(cudaMemcpyAsync(bc_out, dbc, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, s));
-  BC_CUDA(cudaMemcpyAsync(&h_status, W->status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  BC_CUDA(cudaEventRecord(W->ev[3], s));
-  BC_CUDA(cudaStreamSynchronize(s));
+  NPS_CUDA_RETURN(cudaEventRecord(W->ev[2], s));
+  if (!p.device_ptrs) NPS_CUDA_RETURN(cudaMemcpyAsync(bc_out, dbc, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, s));
+  NPS_CUDA_RETURN(cudaMemcpyAsync(&h_status, W->status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  NPS_CUDA_RETURN(cudaEventRecord(W->ev[3], s));
+  NPS_CUDA_RETURN(cudaStreamSynchronize(s));
   if (st) {
     st->status = (int32_t)h_status;
     st->grid_ctas = grid;

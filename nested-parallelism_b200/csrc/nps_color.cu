@@ -453,12 +453,6 @@ __global__ void color_left_kernel(const int32_t* color, int32_t n, uint32_t* lef
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(left, c);
 }
 
-#define CL_CUDA(call)                                                                         \
-  do {                                                                                        \
-    cudaError_t e_ = (call);                                                                  \
-    if (e_ != cudaSuccess)                                                                    \
-      return nps_fail(NPS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
-  } while (0)
 
 struct ColorWork {
   std::mutex mu;
@@ -487,24 +481,6 @@ struct ColorWork {
 std::mutex g_color_mu;
 std::vector<ColorWork*> g_color;
 
-template <class T>
-nps_status ensure(T** p, size_t* have, size_t want, cudaStream_t s) {
-  if (*p && *have >= want) return NPS_OK;
-  if (*p) {
-    cudaStreamSynchronize(s);
-    cudaFree(*p);
-  }
-  *p = nullptr;
-  *have = 0;
-  cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(want, 1) * sizeof(T));
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    *p = nullptr;
-    return nps_fail(NPS_ERR_OOM, std::string("color workspace: cudaMalloc: ") + cudaGetErrorString(e));
-  }
-  *have = want;
-  return NPS_OK;
-}
 
 }  // namespace
 
@@ -527,7 +503,7 @@ extern "C" nps_status nps_color(const int32_t* row_ptr, const int32_t* col, int3
     return nps_fail(NPS_ERR_NO_DEVICE, "no CUDA device");
   }
   if (p.device < 0 || p.device >= dcount) return nps_fail(NPS_ERR_INVALID_ARG, "device ordinal out of range");
-  CL_CUDA(cudaSetDevice(p.device));
+  NPS_CUDA_RETURN(cudaSetDevice(p.device));
   ColorWork* W;
   {
     std::lock_guard<std::mutex> lk(g_color_mu);
@@ -536,28 +512,28 @@ extern "C" nps_status nps_color(const int32_t* row_ptr, const int32_t* col, int3
     W = g_color[p.device];
   }
   std::lock_guard<std::mutex> lk(W->mu);
-  if (!W->stream) CL_CUDA(cudaStreamCreateWithFlags(&W->stream, cudaStreamNonBlocking));
+  if (!W->stream) NPS_CUDA_RETURN(cudaStreamCreateWithFlags(&W->stream, cudaStreamNonBlocking));
   if (!W->ev[0]) {
-    for (auto& ev : W->ev) CL_CUDA(cudaEventCreate(&ev));
+    for (auto& ev : W->ev) NPS_CUDA_RETURN(cudaEventCreate(&ev));
   }
-  if (!W->ctr) CL_CUDA(cudaMalloc((void**)&W->ctr, sizeof(ColorCtr)));
-  if (!W->snap) CL_CUDA(cudaMallocHost((void**)&W->snap, 3 * sizeof(ColorCtr)));
-  if (!W->bar) CL_CUDA(cudaMalloc((void**)&W->bar, 2 * sizeof(uint32_t)));
-  if (!W->sms) CL_CUDA(cudaDeviceGetAttribute(&W->sms, cudaDevAttrMultiProcessorCount, p.device));
+  if (!W->ctr) NPS_CUDA_RETURN(cudaMalloc((void**)&W->ctr, sizeof(ColorCtr)));
+  if (!W->snap) NPS_CUDA_RETURN(cudaMallocHost((void**)&W->snap, 3 * sizeof(ColorCtr)));
+  if (!W->bar) NPS_CUDA_RETURN(cudaMalloc((void**)&W->bar, 2 * sizeof(uint32_t)));
+  if (!W->sms) NPS_CUDA_RETURN(cudaDeviceGetAttribute(&W->sms, cudaDevAttrMultiProcessorCount, p.device));
   cudaStream_t s = p.stream ? (cudaStream_t)p.stream : W->stream;
   if (st) memset(st, 0, sizeof(*st));
   nps_status e;
-  CL_CUDA(cudaEventRecord(W->ev[0], s));
+  NPS_CUDA_RETURN(cudaEventRecord(W->ev[0], s));
   ColorArgs a;
   a.row = row_ptr;
   a.col = col;
   a.color = color_out;
   if (!p.device_ptrs) {
-    if ((e = ensure(&W->row, &W->row_n, (size_t)n + 1, s)) || (e = ensure(&W->col, &W->col_n, (size_t)m, s)) ||
-        (e = ensure(&W->color, &W->color_n, (size_t)n, s)))
+    if ((e = nps_ensure(&W->row, &W->row_n, (size_t)n + 1, s, "color")) || (e = nps_ensure(&W->col, &W->col_n, (size_t)m, s, "color")) ||
+        (e = nps_ensure(&W->color, &W->color_n, (size_t)n, s, "color")))
       return e;
-    CL_CUDA(cudaMemcpyAsync(W->row, row_ptr, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, s));
-    if (m > 0) CL_CUDA(cudaMemcpyAsync(W->col, col, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
+    NPS_CUDA_RETURN(cudaMemcpyAsync(W->row, row_ptr, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, s));
+    if (m > 0) NPS_CUDA_RETURN(cudaMemcpyAsync(W->col, col, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
     a.row = W->row;
     a.col = W->col;
     a.color = W->color;
@@ -566,8 +542,8 @@ extern "C" nps_status nps_color(const int32_t* row_ptr, const int32_t* col, int3
   const size_t nn = (size_t)n;
   // a round cuts at most m / kChunk + m / kHuge + 1 chunks
   const size_t nchunks = (size_t)m / kChunk + (size_t)m / kHuge + 1;
-  if ((e = ensure(&W->buf, &W->buf_n, 4 * nn + 2 + (size_t)nb, s)) || (e = ensure(&W->rcol, &W->rcol_n, (size_t)m, s)) ||
-      (e = ensure(&W->state, &W->state_n, 2 * nn, s)) || (e = ensure(&W->chunk, &W->chunk_n, nchunks, s)))
+  if ((e = nps_ensure(&W->buf, &W->buf_n, 4 * nn + 2 + (size_t)nb, s, "color")) || (e = nps_ensure(&W->rcol, &W->rcol_n, (size_t)m, s, "color")) ||
+      (e = nps_ensure(&W->state, &W->state_n, 2 * nn, s, "color")) || (e = nps_ensure(&W->chunk, &W->chunk_n, nchunks, s, "color")))
     return e;
   a.n = n;
   a.m = m;
@@ -584,39 +560,39 @@ extern "C" nps_status nps_color(const int32_t* row_ptr, const int32_t* col, int3
   a.c = W->ctr;
   const int grid = (int)std::max<int64_t>(
       1, std::min<int64_t>(((int64_t)n + kThreads - 1) / kThreads, (int64_t)W->sms * (2048 / kThreads)));
-  CL_CUDA(cudaMemsetAsync(W->ctr, 0, sizeof(ColorCtr), s));
-  CL_CUDA(cudaMemsetAsync(W->buf, 0, sizeof(int32_t) * (nn + 1), s));  // reverse-list counts
-  CL_CUDA(cudaMemsetAsync(W->state, 0, sizeof(int32_t) * 2 * nn, s));
-  CL_CUDA(cudaEventRecord(W->ev[1], s));
+  NPS_CUDA_RETURN(cudaMemsetAsync(W->ctr, 0, sizeof(ColorCtr), s));
+  NPS_CUDA_RETURN(cudaMemsetAsync(W->buf, 0, sizeof(int32_t) * (nn + 1), s));  // reverse-list counts
+  NPS_CUDA_RETURN(cudaMemsetAsync(W->state, 0, sizeof(int32_t) * 2 * nn, s));
+  NPS_CUDA_RETURN(cudaEventRecord(W->ev[1], s));
   color_count_kernel<<<grid, kThreads, 0, s>>>(a);
   scan_blocks_kernel<<<nb, kThreads, 0, s>>>(a.rrow, n, a.bsum);
   scan_totals_kernel<<<1, kThreads, 0, s>>>(a.bsum, nb, a.rrow + n);
   scan_add_kernel<<<grid, kThreads, 0, s>>>(a.rrow, n, a.bsum, a.rcur);
   color_scatter_kernel<<<grid, kThreads, 0, s>>>(a);
   color_first_kernel<<<grid, kThreads, 0, s>>>(a);
-  CL_CUDA(cudaGetLastError());
+  NPS_CUDA_RETURN(cudaGetLastError());
   // every round in one cooperative launch, as many CTAs as are resident
   int per_sm = 0;
-  CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, color_rounds_kernel, kThreads, 0));
+  NPS_CUDA_RETURN(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, color_rounds_kernel, kThreads, 0));
   // p.ctas_per_sm picks fewer CTAs (cheaper barriers) than the resident maximum
   const int use = p.ctas_per_sm > 0 ? std::min(p.ctas_per_sm, std::max(1, per_sm)) : kRoundCtasPerSm;
   const int rgrid = std::max(1, std::min(W->sms * std::min(use, std::max(1, per_sm)), grid));
-  CL_CUDA(cudaMemsetAsync(W->bar, 0, 2 * sizeof(uint32_t), s));
+  NPS_CUDA_RETURN(cudaMemsetAsync(W->bar, 0, 2 * sizeof(uint32_t), s));
   {
     uint32_t* bar = W->bar;
     uint32_t* abort_word = W->bar + 1;
     unsigned long long timeout_ns = (unsigned long long)(p.timeout_s * 1e9);
     void* args[] = {&a, &bar, &abort_word, &timeout_ns};
-    CL_CUDA(cudaLaunchCooperativeKernel((const void*)color_rounds_kernel, dim3(rgrid), dim3(kThreads), args, 0, s));
+    NPS_CUDA_RETURN(cudaLaunchCooperativeKernel((const void*)color_rounds_kernel, dim3(rgrid), dim3(kThreads), args, 0, s));
   }
-  CL_CUDA(cudaEventRecord(W->ev[2], s));
+  NPS_CUDA_RETURN(cudaEventRecord(W->ev[2], s));
   color_left_kernel<<<grid, kThreads, 0, s>>>(a.color, n, &W->ctr->left);
-  CL_CUDA(cudaGetLastError());
+  NPS_CUDA_RETURN(cudaGetLastError());
   if (!p.device_ptrs)
-    CL_CUDA(cudaMemcpyAsync(color_out, a.color, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost, s));
-  CL_CUDA(cudaMemcpyAsync(&W->snap[2], W->ctr, sizeof(ColorCtr), cudaMemcpyDeviceToHost, s));
-  CL_CUDA(cudaEventRecord(W->ev[3], s));
-  CL_CUDA(cudaStreamSynchronize(s));
+    NPS_CUDA_RETURN(cudaMemcpyAsync(color_out, a.color, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost, s));
+  NPS_CUDA_RETURN(cudaMemcpyAsync(&W->snap[2], W->ctr, sizeof(ColorCtr), cudaMemcpyDeviceToHost, s));
+  NPS_CUDA_RETURN(cudaEventRecord(W->ev[3], s));
+  NPS_CUDA_RETURN(cudaStreamSynchronize(s));
   const ColorCtr& f = W->snap[2];
   if (st) {
     st->status = (int32_t)f.status;

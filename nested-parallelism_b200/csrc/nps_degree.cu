@@ -124,12 +124,6 @@ __global__ void __launch_bounds__(kThreads) degree_pass2(const int32_t* __restri
     if (h[i]) atomicAdd(&dist[i], (unsigned long long)h[i]);
 }
 
-#define DG_CUDA(call)                                                                         \
-  do {                                                                                        \
-    cudaError_t e_ = (call);                                                                  \
-    if (e_ != cudaSuccess)                                                                    \
-      return nps_fail(NPS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
-  } while (0)
 
 // Per-device cached buffers: the staged row_ptr (host-pointer calls), the
 // accumulators and the distribution.
@@ -153,21 +147,6 @@ DegWork* deg_work(int device) {
   return g_deg[device];
 }
 
-template <class T>
-nps_status ensure(T** p, size_t* have, size_t want) {
-  if (*p && *have >= want) return NPS_OK;
-  if (*p) cudaFree(*p);
-  *p = nullptr;
-  *have = 0;
-  cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(want, 1) * sizeof(T));
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    *p = nullptr;
-    return nps_fail(NPS_ERR_OOM, std::string("degree stats: cudaMalloc: ") + cudaGetErrorString(e));
-  }
-  *have = want;
-  return NPS_OK;
-}
 
 }  // namespace
 
@@ -183,40 +162,40 @@ extern "C" nps_status nps_degree_stats(const int32_t* row_ptr, int32_t n, int32_
     return nps_fail(NPS_ERR_NO_DEVICE, "degree stats: no CUDA device");
   }
   if (device < 0 || device >= count) return nps_fail(NPS_ERR_INVALID_ARG, "degree stats: device ordinal out of range");
-  DG_CUDA(cudaSetDevice(device));
+  NPS_CUDA_RETURN(cudaSetDevice(device));
   DegWork* w = deg_work(device);
   std::lock_guard<std::mutex> lk(w->mu);
-  if (!w->stream) DG_CUDA(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking));
+  if (!w->stream) NPS_CUDA_RETURN(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking));
   cudaStream_t s = w->stream;
   nps_status e;
   const int32_t* rp = row_ptr;
   if (!device_ptrs) {
-    if ((e = ensure(&w->rp, &w->rp_n, (size_t)n + 1))) return e;
-    DG_CUDA(cudaMemcpyAsync(w->rp, row_ptr, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, s));
+    if ((e = nps_ensure(&w->rp, &w->rp_n, (size_t)n + 1, s, "degree stats"))) return e;
+    NPS_CUDA_RETURN(cudaMemcpyAsync(w->rp, row_ptr, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, s));
     rp = w->rp;
   }
   size_t one = 0;
   if (!w->acc) {
-    if ((e = ensure(&w->acc, &one, 1))) return e;
+    if ((e = nps_ensure(&w->acc, &one, 1, s, "degree stats"))) return e;
   }
   DegAcc init;
   memset(&init, 0, sizeof(init));
   init.min_key = ~0ull;
-  DG_CUDA(cudaMemcpyAsync(w->acc, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+  NPS_CUDA_RETURN(cudaMemcpyAsync(w->acc, &init, sizeof(init), cudaMemcpyHostToDevice, s));
   int sms = 0;
-  DG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  NPS_CUDA_RETURN(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
   const int blocks = (int)std::min<int64_t>((int64_t)sms * 4, ((int64_t)n + kThreads - 1) / kThreads);
   degree_pass1<<<blocks, kThreads, 0, s>>>(rp, n, w->acc);
-  DG_CUDA(cudaGetLastError());
+  NPS_CUDA_RETURN(cudaGetLastError());
   DegAcc out;
-  DG_CUDA(cudaMemcpyAsync(&out, w->acc, sizeof(out), cudaMemcpyDeviceToHost, s));
-  DG_CUDA(cudaStreamSynchronize(s));
+  NPS_CUDA_RETURN(cudaMemcpyAsync(&out, w->acc, sizeof(out), cudaMemcpyDeviceToHost, s));
+  NPS_CUDA_RETURN(cudaStreamSynchronize(s));
   if (out.bad) return nps_fail(NPS_ERR_FORMAT, "degree stats: row_ptr decreases (malformed CSR)");
 
   memset(info, 0, sizeof(*info));
   info->n = n;
   int32_t m_last = 0;
-  if (device_ptrs) DG_CUDA(cudaMemcpy(&m_last, row_ptr + n, sizeof(int32_t), cudaMemcpyDeviceToHost));
+  if (device_ptrs) NPS_CUDA_RETURN(cudaMemcpy(&m_last, row_ptr + n, sizeof(int32_t), cudaMemcpyDeviceToHost));
   else m_last = row_ptr[n];
   info->m = m_last;
   info->total_degree = (int64_t)out.total;
@@ -237,13 +216,13 @@ extern "C" nps_status nps_degree_stats(const int32_t* row_ptr, int32_t n, int32_
   if (dist_len > 0) {
     if (dist_len < (int64_t)info->max_degree + 1)
       return nps_fail(NPS_ERR_CAPACITY, "degree stats: dist_len must be at least max_degree + 1 (info is filled)");
-    if ((e = ensure(&w->dist, &w->dist_n, (size_t)dist_len))) return e;
-    DG_CUDA(cudaMemsetAsync(w->dist, 0, sizeof(unsigned long long) * (size_t)dist_len, s));
+    if ((e = nps_ensure(&w->dist, &w->dist_n, (size_t)dist_len, s, "degree stats"))) return e;
+    NPS_CUDA_RETURN(cudaMemsetAsync(w->dist, 0, sizeof(unsigned long long) * (size_t)dist_len, s));
     degree_pass2<<<blocks, kThreads, 0, s>>>(rp, n, w->dist, dist_len);
-    DG_CUDA(cudaGetLastError());
-    DG_CUDA(cudaMemcpyAsync(dist, w->dist, sizeof(int64_t) * (size_t)dist_len,
+    NPS_CUDA_RETURN(cudaGetLastError());
+    NPS_CUDA_RETURN(cudaMemcpyAsync(dist, w->dist, sizeof(int64_t) * (size_t)dist_len,
                             device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
-    DG_CUDA(cudaStreamSynchronize(s));
+    NPS_CUDA_RETURN(cudaStreamSynchronize(s));
   }
   return NPS_OK;
 }

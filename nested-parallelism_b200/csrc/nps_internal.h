@@ -2,6 +2,9 @@
 #ifndef NPS_INTERNAL_H_
 #define NPS_INTERNAL_H_
 
+#include <cuda_runtime.h>
+
+#include <algorithm>
 #include <string>
 
 #include "nps.h"
@@ -30,6 +33,37 @@ inline void nps_heavy_items(int64_t m, uint64_t entries, uint64_t cap, uint32_t*
 
 // int4 slots of the grid-tier buffer: hcap entries, then 2 * icap item starts.
 inline size_t nps_heavy_slots(uint32_t hcap, uint32_t icap) { return (size_t)hcap + ((size_t)2 * icap + 3) / 4; }
+
+// Returns NPS_ERR_CUDA, with the call and CUDA's message, when `call` fails.
+#define NPS_CUDA_RETURN(call)                                                                  \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess)                                                                     \
+      return nps_fail(NPS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));       \
+  } while (0)
+
+// Grows the device buffer *p (capacity *have elements) to hold `want` elements:
+// a smaller buffer is freed -- after `s` drains, so no queued work still uses
+// it -- and a new one allocated; its contents are not kept.  NPS_ERR_OOM (naming
+// `what`) when the allocation fails.
+template <class T>
+nps_status nps_ensure(T** p, size_t* have, size_t want, cudaStream_t s, const char* what) {
+  if (*p && *have >= want) return NPS_OK;
+  if (*p) {
+    cudaStreamSynchronize(s);
+    cudaFree(*p);
+  }
+  *p = nullptr;
+  *have = 0;
+  cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(want, 1) * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return nps_fail(NPS_ERR_OOM, std::string(what) + " workspace: cudaMalloc: " + cudaGetErrorString(e));
+  }
+  *have = want;
+  return NPS_OK;
+}
 
 // Device copy of the learned-policy weights of `device` (null if none loaded).
 const void* nps_policy_device_weights(int device);

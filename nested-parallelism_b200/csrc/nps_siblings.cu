@@ -330,12 +330,6 @@ __global__ void __launch_bounds__(kGenThreads) reached_kernel(Graph g, SibCtr* c
   }
 }
 
-#define SB_CUDA(call)                                                                         \
-  do {                                                                                        \
-    cudaError_t e_ = (call);                                                                  \
-    if (e_ != cudaSuccess)                                                                    \
-      return nps_fail(NPS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
-  } while (0)
 
 // Per-device cached workspace.
 struct SibWork {
@@ -373,34 +367,16 @@ SibWork* sib_work(int device) {
   return g_sib[device];
 }
 
-template <class T>
-nps_status ensure(T** p, size_t* have, size_t want, cudaStream_t s) {
-  if (*p && *have >= want) return NPS_OK;
-  if (*p) {
-    cudaStreamSynchronize(s);
-    cudaFree(*p);
-  }
-  *p = nullptr;
-  *have = 0;
-  cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(want, 1) * sizeof(T));
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    *p = nullptr;
-    return nps_fail(NPS_ERR_OOM, std::string("solution workspace: cudaMalloc: ") + cudaGetErrorString(e));
-  }
-  *have = want;
-  return NPS_OK;
-}
 
 nps_status setup(SibWork* W, int device) {
-  if (!W->stream) SB_CUDA(cudaStreamCreateWithFlags(&W->stream, cudaStreamNonBlocking));
-  if (!W->ctr) SB_CUDA(cudaMalloc((void**)&W->ctr, sizeof(SibCtr)));
-  if (!W->snap) SB_CUDA(cudaMallocHost((void**)&W->snap, 3 * sizeof(SibCtr)));
+  if (!W->stream) NPS_CUDA_RETURN(cudaStreamCreateWithFlags(&W->stream, cudaStreamNonBlocking));
+  if (!W->ctr) NPS_CUDA_RETURN(cudaMalloc((void**)&W->ctr, sizeof(SibCtr)));
+  if (!W->snap) NPS_CUDA_RETURN(cudaMallocHost((void**)&W->snap, 3 * sizeof(SibCtr)));
   if (!W->ev[0]) {
-    for (auto& e : W->ev) SB_CUDA(cudaEventCreate(&e));
-    for (auto& e : W->chunk_ev) SB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto& e : W->ev) NPS_CUDA_RETURN(cudaEventCreate(&e));
+    for (auto& e : W->chunk_ev) NPS_CUDA_RETURN(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
-  if (!W->sms) SB_CUDA(cudaDeviceGetAttribute(&W->sms, cudaDevAttrMultiProcessorCount, device));
+  if (!W->sms) NPS_CUDA_RETURN(cudaDeviceGetAttribute(&W->sms, cudaDevAttrMultiProcessorCount, device));
   return NPS_OK;
 }
 
@@ -450,7 +426,7 @@ nps_status enqueue_iteration(const Launch& L, int it, cudaStream_t s) {
     default:
       return nps_fail(NPS_ERR_INVALID_ARG, "solution must be 0..6");
   }
-  SB_CUDA(cudaGetLastError());
+  NPS_CUDA_RETURN(cudaGetLastError());
   return NPS_OK;
 }
 
@@ -479,35 +455,35 @@ nps_status run(SibWork* W, int32_t sol, const Graph& g, const nps_params& p, cud
   L.gen_grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + kGenThreads - 1) / kGenThreads, (int64_t)W->sms * 8));
   L.c = W->ctr;
   nps_status e;
-  if ((e = ensure(&W->q, &W->q_n, (size_t)n, s))) return e;
+  if ((e = nps_ensure(&W->q, &W->q_n, (size_t)n, s, "solution"))) return e;
   L.q = W->q;
   L.buf = nullptr;
   L.slice = 0;
   if (sol == NPS_SOLUTION_GLOBAL_DELAYED) {
-    if ((e = ensure(&W->buf, &W->buf_n, (size_t)n, s))) return e;
+    if ((e = nps_ensure(&W->buf, &W->buf_n, (size_t)n, s, "solution"))) return e;
     L.buf = W->buf;
   } else if (sol == NPS_SOLUTION_NP_OPT) {
     // a CTA sweeps at most bs * ceil(n / (grid * bs)) queue entries
     const int64_t sweeps = (n + (int64_t)L.grid * bs - 1) / ((int64_t)L.grid * bs);
     L.slice = (uint32_t)(sweeps * bs);
-    if ((e = ensure(&W->buf, &W->buf_n, (size_t)L.grid * L.slice, s))) return e;
+    if ((e = nps_ensure(&W->buf, &W->buf_n, (size_t)L.grid * L.slice, s, "solution"))) return e;
     L.buf = W->buf;
   }
   if ((sol == NPS_SOLUTION_NP_NAIVE || sol == NPS_SOLUTION_NP_OPT) && !W->pending_limit) {
     size_t have = 0;
-    SB_CUDA(cudaDeviceGetLimit(&have, cudaLimitDevRuntimePendingLaunchCount));
+    NPS_CUDA_RETURN(cudaDeviceGetLimit(&have, cudaLimitDevRuntimePendingLaunchCount));
     // not fatal: with the default limit more launches are refused and walked by their parent thread
     if (have < kPendingLaunches && cudaDeviceSetLimit(cudaLimitDevRuntimePendingLaunchCount, kPendingLaunches) != cudaSuccess)
       cudaGetLastError();
     W->pending_limit = true;
   }
-  SB_CUDA(cudaMemsetAsync(W->ctr, 0, sizeof(SibCtr), s));
-  SB_CUDA(cudaEventRecord(W->ev[1], s));
+  NPS_CUDA_RETURN(cudaMemsetAsync(W->ctr, 0, sizeof(SibCtr), s));
+  NPS_CUDA_RETURN(cudaEventRecord(W->ev[1], s));
   if (sol == NPS_SOLUTION_DUAL_QUEUE)
     gen_queue_kernel<true><<<L.gen_grid, kGenThreads, 0, s>>>(g, L.q, -1, L.threshold, L.c);
   else
     gen_queue_kernel<false><<<L.gen_grid, kGenThreads, 0, s>>>(g, L.q, -1, L.threshold, L.c);
-  SB_CUDA(cudaGetLastError());
+  NPS_CUDA_RETURN(cudaGetLastError());
 
   // chunks of iterations; the counters of chunk k are read while chunk k + 1 runs
   const int64_t max_iter = 2 * n + 64;
@@ -519,10 +495,10 @@ nps_status run(SibWork* W, int32_t sol, const Graph& g, const nps_params& p, cud
     for (int j = 0; j < chunk; ++j)
       if ((e = enqueue_iteration(L, (int)((it + j) & 1), s))) return e;  // kernels use the parity only
     it += chunk;
-    SB_CUDA(cudaMemcpyAsync(&W->snap[k & 1], W->ctr, sizeof(SibCtr), cudaMemcpyDeviceToHost, s));
-    SB_CUDA(cudaEventRecord(W->chunk_ev[k & 1], s));
+    NPS_CUDA_RETURN(cudaMemcpyAsync(&W->snap[k & 1], W->ctr, sizeof(SibCtr), cudaMemcpyDeviceToHost, s));
+    NPS_CUDA_RETURN(cudaEventRecord(W->chunk_ev[k & 1], s));
     if (k > 0) {
-      SB_CUDA(cudaEventSynchronize(W->chunk_ev[(k - 1) & 1]));
+      NPS_CUDA_RETURN(cudaEventSynchronize(W->chunk_ev[(k - 1) & 1]));
       ++reads;
       const SibCtr& sn = W->snap[(k - 1) & 1];
       const int par = (int)((it - chunk) & 1);  // parity of the first iteration of chunk k
@@ -540,11 +516,11 @@ nps_status run(SibWork* W, int32_t sol, const Graph& g, const nps_params& p, cud
       return nps_fail(NPS_ERR_TIMEOUT, "solution exceeded timeout_s");
     }
   }
-  SB_CUDA(cudaEventRecord(W->ev[2], s));
+  NPS_CUDA_RETURN(cudaEventRecord(W->ev[2], s));
   reached_kernel<<<L.gen_grid, kGenThreads, 0, s>>>(g, L.c);
-  SB_CUDA(cudaGetLastError());
-  SB_CUDA(cudaMemcpyAsync(&W->snap[2], W->ctr, sizeof(SibCtr), cudaMemcpyDeviceToHost, s));
-  SB_CUDA(cudaStreamSynchronize(s));
+  NPS_CUDA_RETURN(cudaGetLastError());
+  NPS_CUDA_RETURN(cudaMemcpyAsync(&W->snap[2], W->ctr, sizeof(SibCtr), cudaMemcpyDeviceToHost, s));
+  NPS_CUDA_RETURN(cudaStreamSynchronize(s));
   const SibCtr& f = W->snap[2];
   if (st) {
     st->iterations = f.iterations;
@@ -574,7 +550,7 @@ nps_status device_setup(int device, SibWork** out) {
     return nps_fail(NPS_ERR_NO_DEVICE, "no CUDA device");
   }
   if (device < 0 || device >= count) return nps_fail(NPS_ERR_INVALID_ARG, "device ordinal out of range");
-  SB_CUDA(cudaSetDevice(device));
+  NPS_CUDA_RETURN(cudaSetDevice(device));
   *out = sib_work(device);
   return NPS_OK;
 }
@@ -605,11 +581,11 @@ extern "C" nps_status nps_sssp_solution_state(int32_t solution, const int32_t* d
   if ((e = setup(W, p.device))) return e;
   cudaStream_t s = p.stream ? (cudaStream_t)p.stream : W->stream;
   if (st) memset(st, 0, sizeof(*st));
-  SB_CUDA(cudaEventRecord(W->ev[0], s));
+  NPS_CUDA_RETURN(cudaEventRecord(W->ev[0], s));
   Graph g{d_row_ptr, d_col, d_w, d_cost, d_update, n, m};
   if ((e = run(W, solution, g, p, s, st, info))) return e;
-  SB_CUDA(cudaEventRecord(W->ev[3], s));
-  SB_CUDA(cudaStreamSynchronize(s));
+  NPS_CUDA_RETURN(cudaEventRecord(W->ev[3], s));
+  NPS_CUDA_RETURN(cudaStreamSynchronize(s));
   if (st) cudaEventElapsedTime(&st->total_ms, W->ev[0], W->ev[3]);
   return NPS_OK;
 }
@@ -637,34 +613,34 @@ extern "C" nps_status nps_sssp_solution(int32_t solution, const int32_t* row_ptr
   if ((e = setup(W, p.device))) return e;
   cudaStream_t s = p.stream ? (cudaStream_t)p.stream : W->stream;
   if (st) memset(st, 0, sizeof(*st));
-  SB_CUDA(cudaEventRecord(W->ev[0], s));
+  NPS_CUDA_RETURN(cudaEventRecord(W->ev[0], s));
   const int32_t *drow = row_ptr, *dcol = col;
   const uint32_t* dw = w;
   uint32_t* ddist = dist_out;
   if (!p.device_ptrs) {
-    if ((e = ensure(&W->row, &W->row_n, (size_t)n + 1, s)) || (e = ensure(&W->col, &W->col_n, (size_t)m, s)) ||
-        (e = ensure(&W->w, &W->w_n, (size_t)m, s)) || (e = ensure(&W->dist, &W->dist_n, (size_t)n, s)))
+    if ((e = nps_ensure(&W->row, &W->row_n, (size_t)n + 1, s, "solution")) || (e = nps_ensure(&W->col, &W->col_n, (size_t)m, s, "solution")) ||
+        (e = nps_ensure(&W->w, &W->w_n, (size_t)m, s, "solution")) || (e = nps_ensure(&W->dist, &W->dist_n, (size_t)n, s, "solution")))
       return e;
-    SB_CUDA(cudaMemcpyAsync(W->row, row_ptr, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, s));
+    NPS_CUDA_RETURN(cudaMemcpyAsync(W->row, row_ptr, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, s));
     if (m > 0) {
-      SB_CUDA(cudaMemcpyAsync(W->col, col, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
-      SB_CUDA(cudaMemcpyAsync(W->w, w, sizeof(uint32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
+      NPS_CUDA_RETURN(cudaMemcpyAsync(W->col, col, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
+      NPS_CUDA_RETURN(cudaMemcpyAsync(W->w, w, sizeof(uint32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
     }
     drow = W->row;
     dcol = W->col;
     dw = W->w;
     ddist = W->dist;
   }
-  if ((e = ensure(&W->upd, &W->upd_n, (size_t)n, s))) return e;
+  if ((e = nps_ensure(&W->upd, &W->upd_n, (size_t)n, s, "solution"))) return e;
   const int ig = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)n + 255) / 256, (int64_t)W->sms * 8));
   init_kernel<<<ig, 256, 0, s>>>(ddist, W->upd, n, src);
-  SB_CUDA(cudaGetLastError());
+  NPS_CUDA_RETURN(cudaGetLastError());
   Graph g{drow, dcol, dw, ddist, W->upd, n, m};
   if ((e = run(W, solution, g, p, s, st, info))) return e;
   if (!p.device_ptrs)
-    SB_CUDA(cudaMemcpyAsync(dist_out, ddist, sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToHost, s));
-  SB_CUDA(cudaEventRecord(W->ev[3], s));
-  SB_CUDA(cudaStreamSynchronize(s));
+    NPS_CUDA_RETURN(cudaMemcpyAsync(dist_out, ddist, sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToHost, s));
+  NPS_CUDA_RETURN(cudaEventRecord(W->ev[3], s));
+  NPS_CUDA_RETURN(cudaStreamSynchronize(s));
   if (st) cudaEventElapsedTime(&st->total_ms, W->ev[0], W->ev[3]);
   return NPS_OK;
 }

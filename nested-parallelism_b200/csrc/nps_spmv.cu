@@ -418,12 +418,6 @@ __global__ void __launch_bounds__(kThreads, kChunkCtas) spmv_chunks_kernel(Mat A
   }
 }
 
-#define SP_CUDA(call)                                                                         \
-  do {                                                                                        \
-    cudaError_t e_ = (call);                                                                  \
-    if (e_ != cudaSuccess)                                                                    \
-      return nps_fail(NPS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
-  } while (0)
 
 struct SpmvWork {
   std::mutex mu;
@@ -453,24 +447,6 @@ struct SpmvWork {
 std::mutex g_spmv_mu;
 std::vector<SpmvWork*> g_spmv;
 
-template <class T>
-nps_status ensure(T** p, size_t* have, size_t want, cudaStream_t s) {
-  if (*p && *have >= want) return NPS_OK;
-  if (*p) {
-    cudaStreamSynchronize(s);
-    cudaFree(*p);
-  }
-  *p = nullptr;
-  *have = 0;
-  cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(want, 1) * sizeof(T));
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    *p = nullptr;
-    return nps_fail(NPS_ERR_OOM, std::string("spmv workspace: cudaMalloc: ") + cudaGetErrorString(e));
-  }
-  *have = want;
-  return NPS_OK;
-}
 
 nps_status spmv_work(int device, SpmvWork** out) {
   int count = 0;
@@ -479,7 +455,7 @@ nps_status spmv_work(int device, SpmvWork** out) {
     return nps_fail(NPS_ERR_NO_DEVICE, "no CUDA device");
   }
   if (device < 0 || device >= count) return nps_fail(NPS_ERR_INVALID_ARG, "device ordinal out of range");
-  SP_CUDA(cudaSetDevice(device));
+  NPS_CUDA_RETURN(cudaSetDevice(device));
   SpmvWork* w;
   {
     std::lock_guard<std::mutex> lk(g_spmv_mu);
@@ -510,27 +486,27 @@ extern "C" nps_status nps_spmv(const int32_t* row_ptr, const int32_t* col, const
   nps_status e = spmv_work(p.device, &W);
   if (e) return e;
   std::lock_guard<std::mutex> lk(W->mu);
-  if (!W->stream) SP_CUDA(cudaStreamCreateWithFlags(&W->stream, cudaStreamNonBlocking));
+  if (!W->stream) NPS_CUDA_RETURN(cudaStreamCreateWithFlags(&W->stream, cudaStreamNonBlocking));
   if (!W->ev[0])
-    for (auto& ev : W->ev) SP_CUDA(cudaEventCreate(&ev));
-  if (!W->ctr) SP_CUDA(cudaMalloc((void**)&W->ctr, sizeof(SpmvCtr)));
-  if (!W->h_ctr) SP_CUDA(cudaMallocHost((void**)&W->h_ctr, sizeof(SpmvCtr)));
-  if (!W->sms) SP_CUDA(cudaDeviceGetAttribute(&W->sms, cudaDevAttrMultiProcessorCount, p.device));
+    for (auto& ev : W->ev) NPS_CUDA_RETURN(cudaEventCreate(&ev));
+  if (!W->ctr) NPS_CUDA_RETURN(cudaMalloc((void**)&W->ctr, sizeof(SpmvCtr)));
+  if (!W->h_ctr) NPS_CUDA_RETURN(cudaMallocHost((void**)&W->h_ctr, sizeof(SpmvCtr)));
+  if (!W->sms) NPS_CUDA_RETURN(cudaDeviceGetAttribute(&W->sms, cudaDevAttrMultiProcessorCount, p.device));
   cudaStream_t s = p.stream ? (cudaStream_t)p.stream : W->stream;
   if (st) memset(st, 0, sizeof(*st));
-  SP_CUDA(cudaEventRecord(W->ev[0], s));
+  NPS_CUDA_RETURN(cudaEventRecord(W->ev[0], s));
   Mat A{row_ptr, col, val, x, y, n, m};
   if (!p.device_ptrs) {
-    if ((e = ensure(&W->row, &W->row_n, (size_t)n + 1, s)) || (e = ensure(&W->col, &W->col_n, (size_t)m, s)) ||
-        (e = ensure(&W->val, &W->val_n, (size_t)m, s)) || (e = ensure(&W->x, &W->x_n, (size_t)n, s)) ||
-        (e = ensure(&W->y, &W->y_n, (size_t)n, s)))
+    if ((e = nps_ensure(&W->row, &W->row_n, (size_t)n + 1, s, "spmv")) || (e = nps_ensure(&W->col, &W->col_n, (size_t)m, s, "spmv")) ||
+        (e = nps_ensure(&W->val, &W->val_n, (size_t)m, s, "spmv")) || (e = nps_ensure(&W->x, &W->x_n, (size_t)n, s, "spmv")) ||
+        (e = nps_ensure(&W->y, &W->y_n, (size_t)n, s, "spmv")))
       return e;
-    SP_CUDA(cudaMemcpyAsync(W->row, row_ptr, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, s));
+    NPS_CUDA_RETURN(cudaMemcpyAsync(W->row, row_ptr, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, s));
     if (m > 0) {
-      SP_CUDA(cudaMemcpyAsync(W->col, col, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
-      SP_CUDA(cudaMemcpyAsync(W->val, val, sizeof(double) * (size_t)m, cudaMemcpyHostToDevice, s));
+      NPS_CUDA_RETURN(cudaMemcpyAsync(W->col, col, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
+      NPS_CUDA_RETURN(cudaMemcpyAsync(W->val, val, sizeof(double) * (size_t)m, cudaMemcpyHostToDevice, s));
     }
-    SP_CUDA(cudaMemcpyAsync(W->x, x, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, s));
+    NPS_CUDA_RETURN(cudaMemcpyAsync(W->x, x, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, s));
     A = Mat{W->row, W->col, W->val, W->x, W->y, n, m};
   }
   const int grid = (int)std::max<int64_t>(
@@ -541,14 +517,14 @@ extern "C" nps_status nps_spmv(const int32_t* row_ptr, const int32_t* col, const
     // large rows <= m / threshold; chunks <= m / kChunk + large rows
     const size_t nl = std::min<size_t>((size_t)n, (size_t)m / (size_t)p.threshold + 1);
     const size_t nc = (size_t)m / kChunk + nl + 1;
-    if ((e = ensure(&W->list, &W->list_n, nl, s)) || (e = ensure(&W->part, &W->part_n, nc, s)) ||
-        (e = ensure(&W->chunks, &W->chunks_n, nc, s)))
+    if ((e = nps_ensure(&W->list, &W->list_n, nl, s, "spmv")) || (e = nps_ensure(&W->part, &W->part_n, nc, s, "spmv")) ||
+        (e = nps_ensure(&W->chunks, &W->chunks_n, nc, s, "spmv")))
       return e;
     L = W->list;
     D = W->chunks;
   }
-  SP_CUDA(cudaMemsetAsync(W->ctr, 0, sizeof(SpmvCtr), s));
-  SP_CUDA(cudaEventRecord(W->ev[1], s));
+  NPS_CUDA_RETURN(cudaMemsetAsync(W->ctr, 0, sizeof(SpmvCtr), s));
+  NPS_CUDA_RETURN(cudaEventRecord(W->ev[1], s));
   switch (p.level) {
     case NPS_LEVEL_WARP:
       spmv_rows_kernel<NPS_LEVEL_WARP><<<grid, kThreads, 0, s>>>(A, p.threshold, L, D, W->ctr);
@@ -558,16 +534,16 @@ extern "C" nps_status nps_spmv(const int32_t* row_ptr, const int32_t* col, const
       break;
     default:
       spmv_rows_kernel<NPS_LEVEL_GRID><<<grid, kThreads, 0, s>>>(A, p.threshold, L, D, W->ctr);
-      SP_CUDA(cudaGetLastError());
+      NPS_CUDA_RETURN(cudaGetLastError());
       spmv_chunks_kernel<<<grid, kThreads, 0, s>>>(A, L, D, W->part, W->ctr);
       break;
   }
-  SP_CUDA(cudaGetLastError());
-  SP_CUDA(cudaEventRecord(W->ev[2], s));
-  if (!p.device_ptrs) SP_CUDA(cudaMemcpyAsync(y, A.y, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s));
-  SP_CUDA(cudaMemcpyAsync(W->h_ctr, W->ctr, sizeof(SpmvCtr), cudaMemcpyDeviceToHost, s));
-  SP_CUDA(cudaEventRecord(W->ev[3], s));
-  SP_CUDA(cudaStreamSynchronize(s));
+  NPS_CUDA_RETURN(cudaGetLastError());
+  NPS_CUDA_RETURN(cudaEventRecord(W->ev[2], s));
+  if (!p.device_ptrs) NPS_CUDA_RETURN(cudaMemcpyAsync(y, A.y, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s));
+  NPS_CUDA_RETURN(cudaMemcpyAsync(W->h_ctr, W->ctr, sizeof(SpmvCtr), cudaMemcpyDeviceToHost, s));
+  NPS_CUDA_RETURN(cudaEventRecord(W->ev[3], s));
+  NPS_CUDA_RETURN(cudaStreamSynchronize(s));
   if (st) {
     st->status = (int32_t)W->h_ctr->status;
     st->grid_ctas = grid;
