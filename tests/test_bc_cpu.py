@@ -55,3 +55,11 @@ def test_source_subsets_fold_in_order(nps, oracle):
     full = oracle.bc(g.row_ptr, g.col)
     assert np.array_equal(oracle.bc(g.row_ptr, g.col, np.arange(g.n)), full)
     assert not np.array_equal(oracle.bc(g.row_ptr, g.col, np.arange(10)), full)
+
+
+def test_bc_arguments_are_checked_before_the_device(nps):
+    g = nps.gen_uniform(100, 500, 10, 1)
+    for sources in ([0, 100], [-1], [5, 99, 1000]):
+        with pytest.raises(nps.NpsError) as ei:
+            nps.bc(g, sources)
+        assert ei.value.status == 1, sources

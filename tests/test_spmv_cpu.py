@@ -56,3 +56,12 @@ def test_spmv_arguments_are_checked(nps):
     g = nps.gen_uniform(100, 500, 10, 1)
     with pytest.raises(ValueError):
         nps.spmv(g, np.ones(3), np.ones(g.n))
+
+
+def test_spmv_levels_and_thresholds_are_checked_before_the_device(nps, oracle):
+    g = nps.gen_uniform(100, 500, 10, 1)
+    val, x = oracle.spmv_data(g.n, g.m)
+    for kw in ({"level": 3}, {"level": -1}, {"threshold": 0}):
+        with pytest.raises(nps.NpsError) as ei:
+            nps.spmv(g, val, x, nps.Params(**kw))
+        assert ei.value.status == 1, kw
