@@ -321,7 +321,8 @@ extern "C" nps_status nps_bc(const int32_t* row_ptr, const int32_t* col, int32_t
   NPS_CUDA_RETURN(cudaMemsetAsync(W->status, 0, sizeof(uint32_t), s));
   NPS_CUDA_RETURN(cudaMemsetAsync(dbc, 0, sizeof(float) * (size_t)n, s));
   if (dsrc && nsrc > 0 && p.device_ptrs) {
-    bc_check_sources_kernel<<<std::min(1024, (nsrc + 255) / 256), 256, 0, s>>>(dsrc, nsrc, n, W->status);
+    bc_check_sources_kernel<<<(int)std::min<int64_t>(1024, ((int64_t)nsrc + 255) / 256), 256, 0, s>>>(dsrc, nsrc, n,
+                                                                                               W->status);
     NPS_CUDA_RETURN(cudaGetLastError());
   }
   BcArgs a;
