@@ -113,8 +113,9 @@ typedef struct nps_params {
   uint32_t delta_schedule;  /* 0: every bucket is delta wide.  Otherwise bucket b (0 = the first)
                                is 2^k wide with k = bits [4b, 4b+4) for b < 7 and bits [28, 32)
                                for every later bucket; delta is then unused (plain policy only) */
-  int32_t reserved[3];      /* reserved[0] = 1: test hook, the first in-kernel barrier waits for an
-                               arrival that never comes, so its bounded wait must expire.
+  int32_t reserved[3];      /* reserved[0] = 1: test hook, the first in-kernel barrier (of the SSSP
+                               kernel, or of nps_color's round kernel) waits for an arrival that
+                               never comes, so its bounded wait must expire.
                                reserved[1] > 0: nps_bc folds at most this many sources per block
                                of dependency rows (0 = as many as 2 GB of rows hold) */
 } nps_params;

@@ -386,15 +386,16 @@ __device__ __forceinline__ uint32_t ld_volatile_u32(const uint32_t* p) {
 // monotonic counter, then a wait for epoch x CTAs arrivals.  The wait is bounded
 // by timeout_ns (then the status becomes NPS_ERR_TIMEOUT and the abort word is
 // set) and ends early when another CTA aborted.  Returns false on either.
+// `extra` raises the target (test hook: an arrival that never comes).
 __device__ bool grid_barrier(uint32_t* bar, uint32_t& epoch, uint32_t ctas, uint32_t* abort_word, uint32_t* status,
-                             unsigned long long timeout_ns) {
+                             unsigned long long timeout_ns, uint32_t extra = 0) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     epoch += 1;
     // the arrival releases this CTA's writes (ordered after the barrier above)
     asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
-    const uint32_t target = epoch * ctas;
+    const uint32_t target = epoch * ctas + extra;
     const unsigned long long t0 = globaltimer_ns();
     int ok = 1;
     while ((int32_t)(ld_volatile_u32(bar) - target) < 0) {
@@ -426,7 +427,7 @@ __device__ bool grid_barrier(uint32_t* bar, uint32_t& epoch, uint32_t ctas, uint
 // counts are read after a barrier, so every CTA sees the same ones and leaves
 // the loop together.
 __global__ void __launch_bounds__(kThreads) color_rounds_kernel(ColorArgs a, uint32_t* bar, uint32_t* abort_word,
-                                                                unsigned long long timeout_ns) {
+                                                                unsigned long long timeout_ns, uint32_t inject) {
   uint32_t epoch = 0;
   for (uint32_t r = 0;; ++r) {
     const int r3 = (int)(r % 3), par = (int)(r & 1);
@@ -438,7 +439,7 @@ __global__ void __launch_bounds__(kThreads) color_rounds_kernel(ColorArgs a, uin
       a.c->rounds += 1;
     }
     round_walk(a, r3, par, len);
-    if (!grid_barrier(bar, epoch, gridDim.x, abort_word, &a.c->status, timeout_ns)) return;
+    if (!grid_barrier(bar, epoch, gridDim.x, abort_word, &a.c->status, timeout_ns, r == 0 ? inject : 0u)) return;
     const uint32_t nc = __ldcg(&a.c->chunks[r3]);
     if (nc) round_chunks(a, r3, par, nc);
     if (!grid_barrier(bar, epoch, gridDim.x, abort_word, &a.c->status, timeout_ns)) return;
@@ -582,7 +583,8 @@ extern "C" nps_status nps_color(const int32_t* row_ptr, const int32_t* col, int3
     uint32_t* bar = W->bar;
     uint32_t* abort_word = W->bar + 1;
     unsigned long long timeout_ns = (unsigned long long)(p.timeout_s * 1e9);
-    void* args[] = {&a, &bar, &abort_word, &timeout_ns};
+    uint32_t inject = p.reserved[0] != 0 ? 1u : 0u;  // test hook: the first barrier cannot complete
+    void* args[] = {&a, &bar, &abort_word, &timeout_ns, &inject};
     NPS_CUDA_RETURN(cudaLaunchCooperativeKernel((const void*)color_rounds_kernel, dim3(rgrid), dim3(kThreads), args, 0, s));
   }
   NPS_CUDA_RETURN(cudaEventRecord(W->ev[2], s));

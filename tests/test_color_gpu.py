@@ -53,3 +53,16 @@ def test_device_pointers_and_malformed_input(nps, oracle, cuda_device):
     with pytest.raises(nps.NpsError) as ei:
         nps.color_device(row, torch.from_numpy(bad.view(np.int32)).to(dev), g.n, g.m, out)
     assert ei.value.status == 7
+
+
+def test_bounded_barrier_wait_times_out_and_context_survives(nps, oracle, cuda_device):
+    """The round kernel's grid barrier gives up after timeout_s: with the test hook its
+    first barrier waits for an arrival that never comes; the call reports
+    NPS_ERR_TIMEOUT and the next call on the same context is exact."""
+    g = nps.gen_rmat(14, 8, seed=2)
+    with pytest.raises(nps.NpsError) as ei:
+        nps.color(g, nps.Params(fault_inject_wait=True, timeout_s=0.2))
+    assert ei.value.status == 4
+    got, st = nps.color(g)
+    want, it = oracle.color(g.row_ptr, g.col)
+    assert np.array_equal(got, want) and st.iterations == it
