@@ -18,7 +18,8 @@ The 12 features (computed in-kernel after each iteration's barrier):
 
 Delta-stepping is exact for any delta and any level, so the policy changes only
 speed; the plain kernel (Params.policy = POLICY_PLAIN, the default) remains the
-fallback and the judge, and distances are identical either way.  A learned call
+fallback and the check of every learned result, and distances are identical
+either way.  A learned call
 on a device without weights loaded is an error, not a silent fallback.
 """
 from __future__ import annotations
