@@ -1007,7 +1007,17 @@ def main():
         n_r, m_r = oracle.reached(g.row_ptr, d0)
         cfg = {"workload": a.workload, "description": desc, "n": g.n, "m": g.m, "m_reached": m_r,
                "source": g.source, "parallelism": "host cores"}
-        print(json.dumps(run_reference(a, nps, g, m_r, n_r, cfg)))
+        line = run_reference(a, nps, g, m_r, n_r, cfg)
+        if oracle.have_reference():
+            # the reference's other CPU path, usssp_cpu (apps/sssp/src/cpu/sssp_kernel.cpp): an OpenMP
+            # frontier sweep on every host thread; its concurrent updates race, so it is reported
+            # with its mismatch count and never used as a result
+            threads = os.cpu_count() or 1
+            du, tu = oracle.ref_usssp_cpu(g.row_ptr, g.col, g.w, g.source, threads=threads)
+            line["usssp_cpu"] = {"value": m_r / tu / 1e9, "unit": "GTEPS", "threads": threads, "seconds": tu,
+                                 "mismatches_vs_dijkstra": int((du != d0).sum()), "exact": False,
+                                 "note": "racy: concurrent unsynchronised updates (non-exact by design)"}
+        print(json.dumps(line))
         return 0
 
     import torch
