@@ -94,7 +94,7 @@ typedef struct nps_params {
   int32_t threshold;        /* degree at which a vertex is consolidated (default 64) */
   int32_t block_threshold;  /* NPS_LEVEL_HYBRID only */
   int32_t grid_threshold;   /* NPS_LEVEL_HYBRID only */
-  int32_t block_size;       /* threads per CTA: 128, 256, 512 or 1024 (default 256) */
+  int32_t block_size;       /* threads per CTA: 128, 256 or 512 (default 256) */
   int32_t ctas_per_sm;      /* resident CTAs per SM; 0 = as many as fit */
   uint32_t delta;           /* near-far bucket width; 0 = unordered frontier (the reference's order) */
   int32_t policy;           /* NPS_POLICY_* */
@@ -232,15 +232,18 @@ nps_status nps_trace_read(int32_t device, nps_trace_rec* out, int32_t cap, int32
 
 /* ---- SSSP without allocation ---------------------------------------------
  * No counterpart in the reference.  For callers that must not allocate device
- * memory during the call (a stream being captured in global mode, a service
- * whose memory is all reserved in its own pool, a host that forbids allocator
- * calls from callbacks): same result as nps_sssp with device pointers, but the
- * kernel's workspace is a file-scope static __device__ array of
- * NPS_NOALLOC_SCRATCH_BYTES that every GPU loading libnps holds until exit.
+ * memory during the call (a service whose memory is all reserved in its own
+ * pool, a host that forbids allocator calls from callbacks): same result as
+ * nps_sssp with device pointers, but the kernel's workspace is a file-scope
+ * static __device__ array of NPS_NOALLOC_SCRATCH_BYTES (10 MiB) that every GPU
+ * loading libnps holds until exit.
  * Limit: n <= NPS_NOALLOC_MAX_VERTICES (larger graphs get NPS_ERR_CAPACITY).
- * The first call on a device resolves the array's address (call it once before
- * any stream capture).  Calls share the array: calls whose kernels overlap on the
- * GPU race, so order them on one stream.  No trace, no kernel_ms in the stats.
+ * The call synchronises its stream to return a status, so it cannot run on a
+ * stream being captured into a CUDA graph (NPS_ERR_INVALID_ARG there).  The
+ * first call on a device resolves the array's address and caches it; a
+ * cudaDeviceReset() of that device invalidates the cached address.  Calls share
+ * the array: calls whose kernels overlap on the GPU race, so order them on one
+ * stream.  No trace, no kernel_ms in the stats.
  * Device pointers only; p->stream selects the stream (NULL = legacy default). */
 #define NPS_NOALLOC_MAX_VERTICES 131072
 #define NPS_NOALLOC_SCRATCH_BYTES (10u << 20)

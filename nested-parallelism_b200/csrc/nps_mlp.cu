@@ -87,8 +87,29 @@ __device__ __forceinline__ float ce_head(const float* o, int n, int label, float
   return scale * (lz - o[label]);
 }
 
+// Butterfly transpose-sum over a warp: on return lane L holds the sum over all
+// 32 lanes of v[L].  31 shuffles for 32 sums (v is overwritten).
+__device__ __forceinline__ float transpose_sum32(float (&v)[32], int lane) {
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) {
+    const bool hi = (lane & off) != 0;
+#pragma unroll
+    for (int i = 0; i < off; ++i) {
+      const float send = hi ? v[i] : v[i + off];
+      const float keep = hi ? v[i + off] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+    }
+  }
+  return v[0];
+}
+
 // Mean weighted cross-entropy of both heads; gradients accumulate (fp32) into
 // g_* which the caller zeroes.  Labels < 0 drop that head for the sample.
+// One sample per lane.  A warp's 32 per-sample outer products are summed with
+// transpose-sums, so lane j ends up owning hidden unit j's gradients (column j
+// of w2, row j of w1, b1[j]; lane k < 14 also b2[k]) and adds them to the CTA's
+// shared accumulators without contention inside the warp.
+static_assert(HID == 32 && OUT <= 32, "one lane per hidden unit");
 __global__ void mlp_loss_backward_kernel(const uint16_t* w1, const float* b1, const uint16_t* w2,
                                          const float* b2, const float* X, const int32_t* yd,
                                          const int32_t* yl, const float* wt, int B, float inv_wsum,
@@ -103,31 +124,57 @@ __global__ void mlp_loss_backward_kernel(const uint16_t* w1, const float* b1, co
   for (int i = threadIdx.x; i < OUT; i += blockDim.x) g.b2[i] = 0.f;
   if (threadIdx.x == 0) sl = 0.f;
   __syncthreads();
+  const int lane = threadIdx.x & 31;
   float my_loss = 0.f;
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < B; r += gridDim.x * blockDim.x) {
+  // the bound is uniform per warp: every lane takes part in the transpose-sums
+  for (int r0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); r0 < B; r0 += gridDim.x * blockDim.x) {
+    const int r = r0 + lane;
+    const bool act = r < B;
     float x[IN], h[HID], o[OUT], d[OUT];
 #pragma unroll
-    for (int i = 0; i < IN; ++i) x[i] = X[(size_t)r * IN + i];
+    for (int i = 0; i < IN; ++i) x[i] = act ? X[(size_t)r * IN + i] : 0.f;
     forward_one(s, x, h, o);
-    const float sc = (wt ? wt[r] : 1.f) * inv_wsum;
-    for (int k = 0; k < OUT; ++k) d[k] = 0.f;
-    if (yd[r] >= 0 && yd[r] < ND) my_loss += ce_head(o, ND, yd[r], sc, d);
-    if (yl[r] >= 0 && yl[r] < NL) my_loss += ce_head(o + ND, NL, yl[r], sc, d + ND);
-    float dh[HID];
-    for (int j = 0; j < HID; ++j) dh[j] = 0.f;
-    for (int k = 0; k < OUT; ++k) {
-      if (d[k] == 0.f) continue;
-      atomicAdd(&g.b2[k], d[k]);
-      for (int j = 0; j < HID; ++j) {
-        if (h[j] != 0.f) atomicAdd(&g.w2[k * HID + j], d[k] * h[j]);
-        dh[j] = fmaf(s.w2[k * HID + j], d[k], dh[j]);
-      }
-    }
-    for (int j = 0; j < HID; ++j) {
-      if (h[j] <= 0.f || dh[j] == 0.f) continue;  // ReLU gate
-      atomicAdd(&g.b1[j], dh[j]);
 #pragma unroll
-      for (int i = 0; i < IN; ++i) atomicAdd(&g.w1[j * IN + i], dh[j] * x[i]);
+    for (int k = 0; k < OUT; ++k) d[k] = 0.f;
+    if (act) {
+      const float sc = (wt ? wt[r] : 1.f) * inv_wsum;
+      if (yd[r] >= 0 && yd[r] < ND) my_loss += ce_head(o, ND, yd[r], sc, d);
+      if (yl[r] >= 0 && yl[r] < NL) my_loss += ce_head(o + ND, NL, yl[r], sc, d + ND);
+    }
+    float v[32];
+    // b2: lanes 0..OUT-1
+#pragma unroll
+    for (int k = 0; k < 32; ++k) v[k] = k < OUT ? d[k] : 0.f;
+    const float gb2 = transpose_sum32(v, lane);
+    if (lane < OUT && gb2 != 0.f) atomicAdd(&g.b2[lane], gb2);
+    // w2[k][j] += d[k] h[j]: lane j owns column j
+#pragma unroll 1
+    for (int k = 0; k < OUT; ++k) {
+#pragma unroll
+      for (int j = 0; j < HID; ++j) v[j] = d[k] * h[j];
+      const float t = transpose_sum32(v, lane);
+      if (t != 0.f) atomicAdd(&g.w2[k * HID + lane], t);
+    }
+    // back through the ReLU: dh[j] = (h[j] > 0) * sum_k w2[k][j] d[k]
+    float dh[HID];
+#pragma unroll
+    for (int j = 0; j < HID; ++j) {
+      float a = 0.f;
+#pragma unroll
+      for (int k = 0; k < OUT; ++k) a = fmaf(s.w2[k * HID + j], d[k], a);
+      dh[j] = h[j] > 0.f ? a : 0.f;
+    }
+#pragma unroll
+    for (int j = 0; j < HID; ++j) v[j] = dh[j];
+    const float gb1 = transpose_sum32(v, lane);
+    if (gb1 != 0.f) atomicAdd(&g.b1[lane], gb1);
+    // w1[j][i] += dh[j] x[i]: lane j owns row j
+#pragma unroll 1
+    for (int i = 0; i < IN; ++i) {
+#pragma unroll
+      for (int j = 0; j < HID; ++j) v[j] = dh[j] * x[i];
+      const float t = transpose_sum32(v, lane);
+      if (t != 0.f) atomicAdd(&g.w1[lane * IN + i], t);
     }
   }
   atomicAdd(&sl, my_loss);

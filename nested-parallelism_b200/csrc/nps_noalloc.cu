@@ -1,23 +1,29 @@
 // nps_sssp_noalloc(): single-source shortest paths without any allocation.
 //
 // Who needs it.  Some callers cannot allocate device memory at the moment they
-// want a shortest-path answer: code running while a stream is being captured
-// into a CUDA graph in global capture mode (cudaMalloc is an error there);
-// services that reserve all device memory up front in their own pool and must
-// not let a library grow its footprint or stall other streams with a
-// device-synchronising allocation; and plug-in hosts that forbid allocator
-// calls from callbacks.  The regular entry points keep a per-context workspace
-// that grows with cudaMalloc the first time a larger graph arrives; this one
-// never calls cudaMalloc, cudaFree, cudaMallocHost, stream or event creation.
+// want a shortest-path answer: services that reserve all device memory up front
+// in their own pool and must not let a library grow its footprint or stall
+// other streams with a device-synchronising cudaMalloc, and plug-in hosts that
+// forbid allocator calls from their callbacks.  The regular entry points keep a
+// per-context workspace that grows with cudaMalloc the first time a larger
+// graph arrives; this one never calls cudaMalloc, cudaFree, cudaMallocHost,
+// stream or event creation.
+//
+// Not for stream capture.  The call waits for its kernel (it copies the run's
+// counters to the host and synchronises the stream to return a status), which a
+// stream being captured into a CUDA graph does not allow; on a capturing stream
+// it returns NPS_ERR_INVALID_ARG before doing anything.
 //
 // How.  The workspace the persistent kernel needs (queues, dedupe stamps, the
 // grid-tier list, counters, barrier words) lives in one file-scope
-// `static __device__` array, NPS_NOALLOC_SCRATCH_BYTES long, sized for graphs of
-// up to NPS_NOALLOC_MAX_VERTICES vertices (edges are not limited).  Every GPU that loads libnps holds
-// this array until the process exits.  The array's host-side name is only a
-// stand-in for the symbol, not a device address, so the first call on each
-// device resolves the address with cudaGetSymbolAddress (that device current)
-// and caches it; make that first call before any stream capture begins.
+// `static __device__` array of NPS_NOALLOC_SCRATCH_BYTES (10 MiB), sized for
+// graphs of up to NPS_NOALLOC_MAX_VERTICES vertices (edges are not limited).
+// Every GPU that loads libnps holds this array until the process exits.  The
+// array's host-side name is only a stand-in for the symbol, not a device
+// address, so the first call on each device resolves the address with
+// cudaGetSymbolAddress (that device current) and caches it for the life of the
+// process.  cudaDeviceReset() unloads the module and invalidates that address:
+// do not use this entry point after resetting a device it has run on.
 //
 // Sharing.  All calls on a device share the one array and it keeps the state of
 // the last call: counters and barrier words are cleared at the start of each
@@ -64,9 +70,10 @@ static_assert(kScratchBytes <= NPS_NOALLOC_SCRATCH_BYTES, "scratch layout exceed
 
 }  // namespace
 
-// The scratch.  Host code must not take its address directly (that would be
+// The scratch, NPS_NOALLOC_SCRATCH_BYTES long (the layout above uses the first
+// kScratchBytes).  Host code must not take its address directly (that would be
 // the host shadow, not device memory); see scratch_address().
-static __device__ __align__(256) unsigned char g_nps_noalloc_scratch[kScratchBytes];
+static __device__ __align__(256) unsigned char g_nps_noalloc_scratch[NPS_NOALLOC_SCRATCH_BYTES];
 
 namespace {
 
@@ -143,6 +150,13 @@ extern "C" nps_status nps_sssp_noalloc(const int32_t* d_row_ptr, const int32_t* 
 
   DeviceGuard guard;
   NA_CUDA(cudaSetDevice(p.device));
+  cudaStream_t s = (cudaStream_t)p.stream;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  NA_CUDA(cudaStreamIsCapturing(s, &cap));
+  if (cap != cudaStreamCaptureStatusNone)
+    return nps_fail(NPS_ERR_INVALID_ARG,
+                    "noalloc: the stream is being captured; this call synchronises the stream to return its "
+                    "status, which a capture does not allow");
   int major = 0, sms = 0, coop = 0;
   NA_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, p.device));
   NA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device));
@@ -163,7 +177,6 @@ extern "C" nps_status nps_sssp_noalloc(const int32_t* d_row_ptr, const int32_t* 
   const size_t stride = 32 * (2 + (size_t)(grid + nps::kBarGroup - 1) / nps::kBarGroup);
   if (stride > kBarWords) return nps_fail(NPS_ERR_CAPACITY, "noalloc: too many CTAs for the barrier area");
 
-  cudaStream_t s = (cudaStream_t)p.stream;
   Counters* ctr = (Counters*)(base + kOffCtr);
   uint32_t* marks = (uint32_t*)(base + kOffMarks);
   int32_t* queues = (int32_t*)(base + kOffQueues);

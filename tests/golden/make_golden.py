@@ -122,7 +122,7 @@ def analyzer_goldens():
     statistics and degree distribution."""
     import tempfile
     if not oracle.have_analyzer():
-        sys.exit("oracle/_ref/analyzer missing: build it with `make -C oracle` where the reference exists")
+        sys.exit("oracle/_ref/analyzer missing: build it with `make -C oracle NPS_REFERENCE=<reference checkout>`")
     res = {}
     for fname, fmt in (("reader_dimacs9.gr", 0), ("reader_dimacs10.graph", 1), ("reader_slndc.txt", 2)):
         r = oracle.ref_analyzer(os.path.join(HERE, fname), fmt)
@@ -143,7 +143,7 @@ def bfs_goldens():
     """Levels from the reference's bfs_cpu on every case graph (FNV-1a of the int32
     levels viewed as uint32) and on the edge cases (the levels themselves)."""
     if not oracle.have_reference_bfs():
-        sys.exit("oracle/_ref/libref_bfs.so missing: build it with `make -C oracle` where the reference exists")
+        sys.exit("oracle/_ref/libref_bfs.so missing: build it with `make -C oracle NPS_REFERENCE=<reference checkout>`")
     res = {"cases": {}, "edge_cases": {}}
     for name, kind, args, src in CASES:
         g = gen(kind, args)
@@ -163,7 +163,7 @@ def spmv_goldens():
     """y from the reference's spmv_omp on its own data for every case graph (FNV-1a
     of the float64 bits) and on the edge cases (the values themselves)."""
     if not oracle.have_reference_spmv():
-        sys.exit("oracle/_ref/libref_spmv.so missing: build it with `make -C oracle` where the reference exists")
+        sys.exit("oracle/_ref/libref_spmv.so missing: build it with `make -C oracle NPS_REFERENCE=<reference checkout>`")
     res = {"cases": {}, "edge_cases": {}}
     for name, kind, args, _ in CASES:
         g = gen(kind, args)
@@ -188,7 +188,7 @@ def bc_goldens():
     """Centralities from the reference's bc_cpu (every vertex a source, one thread):
     FNV-1a of the float32 bits per graph, and the values for the edge cases."""
     if not oracle.have_reference_bc():
-        sys.exit("oracle/_ref/libref_bc.so missing: build it with `make -C oracle` where the reference exists")
+        sys.exit("oracle/_ref/libref_bc.so missing: build it with `make -C oracle NPS_REFERENCE=<reference checkout>`")
     res = {"cases": {}, "edge_cases": {}}
     for name, kind, args in BC_GRAPHS:
         g = gen(kind, args)
@@ -204,7 +204,7 @@ def bc_goldens():
 
 def main():
     if not oracle.have_reference():
-        sys.exit("oracle/_ref/libref_sssp.so missing: build it with `make -C oracle` where the reference exists")
+        sys.exit("oracle/_ref/libref_sssp.so missing: build it with `make -C oracle NPS_REFERENCE=<reference checkout>`")
     out = {"generator": "nested-parallelism_b200 seeded generators (splitmix64 counter streams)",
            "expected_by": "reference SSSP_CPU (apps/sssp/src/cpu/sssp.cpp) built from its sources",
            "cases": {}, "edge_cases": {}, "readers": {}}
