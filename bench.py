@@ -48,8 +48,9 @@ sys.path.insert(0, ROOT)
 
 WORKLOADS = {
     # name: (kind, args, description)
-    "rmat22": ("rmat", dict(scale=22, edge_factor=16, seed=1000),
-               "R-MAT scale 22, edge factor 16, a=.57 b=.19 c=.19, w in [1,255], seed 1000, deduped"),
+    "rmat22": ("rmat_eval", dict(scale=22, edge_factor=16, seeds=tuple(range(1000, 1010)), tune_seed=999),
+               "R-MAT scale 22, edge factor 16, a=.57 b=.19 c=.19, w in [1,255], deduped, source = highest "
+               "out-degree vertex; the learned policy's ten held-out evaluation graphs, seeds 1000-1009"),
     "rmat20": ("rmat", dict(scale=20, edge_factor=16, seed=1),
                "R-MAT scale 20, edge factor 16, a=.57 b=.19 c=.19, w in [1,255], seed 1, deduped"),
     "grid4096": ("grid", dict(rows=4096, cols=4096, drop=0.05, wmax=1000, seed=1),
@@ -958,6 +959,387 @@ def bench_color(a, nps, ws, rank, local, desc):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# The default workload: R-MAT scale 22 on the learned policy's ten held-out
+# evaluation seeds.  CPU work runs in spawned processes that build each graph
+# with the oracle's restatement of the generator (identical arrays, checked by
+# tests/test_oracle_cpu.py), so no CPU process ever loads the library.
+
+def _rmat_cpu_worker(scale, ef, seed, reps, use_ref, q, go, timeout_s):
+    """One host process: build R-MAT (scale, ef, seed), report ready, wait for `go`,
+    then run `reps` single-source searches by the reference's SSSP_CPU (oracle/_ref)
+    or, without it, the oracle's restatement; report the distance hash and times."""
+    os.environ["OMP_NUM_THREADS"] = "1"  # one core per process
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    try:
+        row, col, w, src = oracle.gen_rmat(scale, ef, seed)
+        q.put(("ready", seed))
+        if not go.wait(timeout_s):
+            q.put(("error", seed, "start signal never came"))
+            return
+        times, d = [], None
+        for _ in range(reps):
+            if use_ref:
+                d, t = oracle.ref_sssp_cpu(row, col, w, src)
+            else:
+                d, t = oracle.timed(oracle.sssp_heap, row, col, w, src)
+            times.append(t)
+        n_r, m_r = oracle.reached(row, d)
+        q.put(("done", seed, oracle.fnv1a(d), times, n_r, m_r, src, int(row.shape[0] - 1), int(col.shape[0])))
+    except Exception as e:  # reported to the parent, which fails loudly
+        q.put(("error", seed, repr(e)))
+
+
+class CpuSearches:
+    """Spawned processes, one per (seed, repetitions): each builds its graph, and all
+    start their searches together once every graph is built (synchronized) or as
+    soon as their own is (not synchronized)."""
+
+    def __init__(self, scale, ef, seed_reps, use_ref, synchronized, timeout_s=1800):
+        import multiprocessing as mp
+        ctx = mp.get_context("spawn")
+        self.q, self.go = ctx.Queue(), ctx.Event()
+        self.synchronized = synchronized
+        if not synchronized:
+            self.go.set()
+        self.procs = [ctx.Process(target=_rmat_cpu_worker,
+                                  args=(scale, ef, sd, r, use_ref, self.q, self.go, timeout_s), daemon=True)
+                      for sd, r in seed_reps]
+        for pr in self.procs:
+            pr.start()
+        self.timeout_s = timeout_s
+        self.wall = None
+        self.results = {}
+
+    def _get(self):
+        """Next message; fails loudly when a process died without answering or the
+        whole set ran past its time bound."""
+        import queue
+        t_end = time.perf_counter() + self.timeout_s
+        while True:
+            try:
+                msg = self.q.get(timeout=5)
+                break
+            except queue.Empty:
+                dead = [pr for pr in self.procs if pr.exitcode not in (None, 0)]
+                if dead:
+                    raise RuntimeError(f"a CPU search process exited with code {dead[0].exitcode}")
+                if time.perf_counter() > t_end:
+                    raise RuntimeError("CPU search processes did not answer in time")
+        if msg[0] == "error":
+            raise RuntimeError(f"CPU search for seed {msg[1]} failed: {msg[2]}")
+        return msg
+
+    def start(self):
+        """Wait until every graph is built, then start all searches; returns when they end."""
+        ready = 0
+        while ready < len(self.procs):
+            if self._get()[0] == "ready":
+                ready += 1
+        t0 = time.perf_counter()
+        self.go.set()
+        self.collect()
+        self.wall = time.perf_counter() - t0
+        return self.results
+
+    def collect(self):
+        while len(self.results) < len(self.procs):
+            msg = self._get()
+            if msg[0] == "done":
+                _, seed, h, times, n_r, m_r, src, n, m = msg
+                self.results[seed] = dict(fnv=h, times=times, n_r=n_r, m_r=m_r, source=src, n=n, m=m)
+        for pr in self.procs:
+            pr.join(timeout=60)
+        return self.results
+
+
+def _cpu_use_ref():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    return oracle.have_reference()
+
+
+def rmat_eval_config(wl, desc, seeds, per_seed):
+    """The config block both arms print for the evaluation workload."""
+    return {"workload": wl, "description": desc, "scale": WORKLOADS[wl][1]["scale"],
+            "edge_factor": WORKLOADS[wl][1]["edge_factor"], "seeds": list(seeds),
+            "n": per_seed[seeds[0]]["n"], "m_per_seed": [per_seed[sd]["m"] for sd in seeds],
+            "m_reached_per_seed": [per_seed[sd]["m_r"] for sd in seeds],
+            "step": f"one SSSP from the source of each of the {len(seeds)} graphs",
+            "l2": "flushed before every SSSP (256 MB write); the 12 B/edge CSR also exceeds L2"}
+
+
+def reference_rmat_eval(a, wl, desc):
+    """--impl reference on the evaluation workload: the reference's SSSP_CPU on the
+    host cores, one process per graph, all searches started together; a step = one
+    SSSP of each graph (the arm's K steps are K searches per graph)."""
+    _, w, _ = WORKLOADS[wl]
+    seeds = a.seeds or w["seeds"]
+    use_ref = _cpu_use_ref()
+    cores = os.cpu_count() or 1
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except Exception:
+        avail = 64 << 30
+    per_proc = (w["edge_factor"] << w["scale"]) * 40 + (256 << 20)  # generator peak, bytes
+    procs = max(1, min(len(seeds), cores, int(avail * 0.6 // per_proc)))
+    seeds = list(seeds)[:procs] if procs < len(seeds) else list(seeds)
+    cs = CpuSearches(w["scale"], w["edge_factor"], [(sd, a.steps) for sd in seeds], use_ref, synchronized=True)
+    res = cs.start()
+    wall = cs.wall
+    total_edges = a.steps * sum(res[sd]["m_r"] for sd in seeds)
+    value = total_edges / wall / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * wall / a.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic", "config": rmat_eval_config(wl, desc, seeds, res),
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": len(seeds),
+                         "kind": "reference" if use_ref else "port",
+                         "sample": f"every step: one full SSSP of each of the {len(seeds)} graphs, one process "
+                                   "(one core) per graph, all started together; "
+                                   + ("the reference's SSSP_CPU (apps/sssp/src/cpu/sssp.cpp) built from its "
+                                      "sources" if use_ref else "the oracle's restatement of SSSP_CPU")},
+        "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "per_seed_seconds": {str(sd): res[sd]["times"] for sd in seeds},
+        "warmup_note": "warm-up = every process builds its graph and loads the reference code before the "
+                       "timed searches start",
+    }
+    if use_ref:
+        # the reference's other CPU path, usssp_cpu (apps/sssp/src/cpu/sssp_kernel.cpp): an OpenMP frontier
+        # sweep on every host thread, on the first graph; its concurrent updates race, so it is reported with
+        # its mismatch count and never used as a result
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        row, col, wt, src = oracle.gen_rmat(w["scale"], w["edge_factor"], seeds[0])
+        d0, _ = oracle.ref_sssp_cpu(row, col, wt, src)
+        du, tu = oracle.ref_usssp_cpu(row, col, wt, src, threads=cores)
+        line["usssp_cpu"] = {"value": res[seeds[0]]["m_r"] / tu / 1e9, "unit": "GTEPS", "threads": cores,
+                             "seconds": tu, "seed": seeds[0], "mismatches_vs_dijkstra": int((du != d0).sum()),
+                             "exact": False, "note": "racy: concurrent unsynchronised updates (non-exact by design)"}
+    return line
+
+
+def bench_rmat_eval(a, ws, rank, local, wl, desc):
+    """Our arm on the evaluation workload: the plain autotuned kernel and the learned
+    policy on every evaluation graph, each SSSP checked against the reference's CPU
+    Dijkstra run in spawned processes while the GPU works."""
+    _, w, _ = WORKLOADS[wl]
+    seeds = list(a.seeds or w["seeds"])
+    cpu = None
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        # started before the first CUDA call (spawned processes, no library loaded)
+        cpu = CpuSearches(w["scale"], w["edge_factor"], [(sd, 1) for sd in seeds], _cpu_use_ref(),
+                          synchronized=False)
+    nps = importlib.import_module("nested-parallelism_b200")
+    import torch
+    import torch.distributed as dist
+    if ws > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    at = importlib.import_module("nested-parallelism_b200.autotune")
+    pol = importlib.import_module("nested-parallelism_b200.policy")
+
+    # ---- configuration: the autotuner runs on a graph of the same shape that is not an
+    # evaluation graph (seed tune_seed), outside any timed region
+    prm = dict(DEFAULT_PARAMS["rmat"])
+    if a.delta is not None:
+        prm["delta"] = a.delta
+    if a.level is not None:
+        prm["level"] = a.level
+    wpath = os.path.join(ROOT, "nested-parallelism_b200", "policy_weights.npz")
+    use_learned = a.policy == "learned" and os.path.exists(wpath)
+    if use_learned:
+        pol.load_into_kernel(pol.MLPWeights.load(wpath), local)
+    tune_log = []
+    plain = nps.Params(device=local, **prm)
+    learned = dataclasses.replace(plain, policy=nps.POLICY_LEARNED, light_heavy=False, order_degree=0,
+                                  delta_schedule=0) if use_learned else None
+    if a.tune_budget > 0 and a.delta is None and a.level is None:
+        gt = nps.gen_rmat(w["scale"], w["edge_factor"], seed=w["tune_seed"])
+        dgt = at.to_device(gt, device=dev)
+        plain, _, tune_log = at.autotune([dgt], repeats=3, budget=a.tune_budget, seed=plain)
+        plain.device = local
+        if use_learned:
+            learned = dataclasses.replace(plain, policy=nps.POLICY_LEARNED, light_heavy=False, order_degree=0,
+                                          delta_schedule=0)
+            learned, _, ltune = at.autotune([dgt], repeats=3, budget=LEARNED_TUNE_BUDGET, seed=learned,
+                                            axes=LEARNED_AXES)
+            learned.device = local
+            tune_log = tune_log + ltune
+        del dgt, gt
+    params = learned if use_learned else plain
+
+    # ---- the evaluation graphs, resident on the device
+    graphs = []
+    for sd in seeds:
+        g = nps.gen_rmat(w["scale"], w["edge_factor"], seed=sd)
+        graphs.append((sd, g, at.to_device(g, device=dev)))
+    flush = torch.empty(256 << 20, dtype=torch.int8, device=dev)  # > 126 MB L2
+    stream = torch.cuda.Stream(dev)
+    sptr = stream.cuda_stream
+
+    def timed(p, clk=None):
+        """W warm-up SSSPs per graph, then K steps of one SSSP per graph, the L2 flushed
+        before each; CUDA events on the launch stream around every SSSP."""
+        with torch.cuda.stream(stream):
+            for _ in range(a.warmup):
+                for _, g, dg in graphs:
+                    nps.sssp_device(dg.row_ptr, dg.col, dg.w, g.n, g.m, g.source, dg.dist, p, stream=sptr)
+        torch.cuda.synchronize(dev)
+        evs = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                for _ in graphs] for _ in range(a.steps)]
+        stats = [None] * len(graphs)
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        ctx = clk if clk is not None else contextlib.nullcontext()
+        with ctx:
+            with torch.cuda.stream(stream):
+                for i in range(a.steps):
+                    for j, (_, g, dg) in enumerate(graphs):
+                        flush.fill_((i * len(graphs) + j) & 0x7F)
+                        evs[i][j][0].record(stream)
+                        stats[j] = nps.sssp_device(dg.row_ptr, dg.col, dg.w, g.n, g.m, g.source, dg.dist, p,
+                                                   stream=sptr)
+                        evs[i][j][1].record(stream)
+                torch.cuda.synchronize(dev)
+        if ws > 1:
+            dist.barrier()
+        ms = [[evs[i][j][0].elapsed_time(evs[i][j][1]) for i in range(a.steps)] for j in range(len(graphs))]
+        return ms, stats
+
+    def distances(p):
+        out = []
+        for _, g, dg in graphs:
+            nps.sssp_device(dg.row_ptr, dg.col, dg.w, g.n, g.m, g.source, dg.dist, p)
+            out.append(dg.dist.cpu().numpy().view(np.uint32).copy())
+        return out
+
+    plain_ms, plain_stats = timed(plain)
+    d_plain = distances(plain)
+    per = {}
+    for j, (sd, g, _) in enumerate(graphs):
+        reached = d_plain[j] < nps.INF
+        n_r = int(reached.sum())
+        m_r = int(np.diff(g.row_ptr)[reached].sum())
+        per[sd] = dict(n=g.n, m=g.m, m_r=m_r, n_r=n_r, source=g.source, b_alg=12 * m_r + 12 * n_r + 4 * g.n)
+    clk = ClockSampler(local)
+    step_ms, stats = timed(params, clk)
+    clocks = clk.summary()
+    d_head = distances(params)
+    exact_vs_plain = all(np.array_equal(x, y) for x, y in zip(d_head, d_plain))
+
+    # ---- e2e: the public host-buffer call, pinned host CSR in, distances out, every SSSP
+    def pinned(x):
+        return torch.from_numpy(np.ascontiguousarray(x).view(np.int32)).pin_memory().numpy()
+    hosts = [(nps.Graph(pinned(g.row_ptr), pinned(g.col), pinned(g.w).view(np.uint32), g.source),
+              torch.empty(g.n, dtype=torch.int32).pin_memory().numpy().view(np.uint32)) for _, g, _ in graphs]
+    e2e_steps = a.e2e_steps or 1
+    nps.sssp(hosts[0][0], None, params, out=hosts[0][1])
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for hg, hout in hosts:
+            nps.sssp(hg, None, params, out=hout)  # synchronous: H2D + kernel + D2H
+    e2e_wall = time.perf_counter() - t0
+    e2e_ok = all(np.array_equal(hout, d) for (_, hout), d in zip(hosts, d_head))
+    del hosts
+
+    seed_ms = [sum(x) for x in step_ms]             # per graph, over K steps
+    plain_seed_ms = [sum(x) for x in plain_ms]
+    kern_ms = sum(seed_ms)
+    tot_t = torch.tensor([kern_ms, e2e_wall * 1e3, sum(plain_seed_ms)], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(tot_t, op=dist.ReduceOp.MAX)
+    kern_ms_max, e2e_ms_max, plain_ms_max = float(tot_t[0]), float(tot_t[1]), float(tot_t[2])
+    mr = [per[sd]["m_r"] for sd in seeds]
+    gteps = [a.steps * m / (t * 1e-3) / 1e9 for m, t in zip(mr, seed_ms)]
+    plain_gteps = [a.steps * m / (t * 1e-3) / 1e9 for m, t in zip(mr, plain_seed_ms)]
+    geo = float(np.exp(np.mean(np.log(gteps))))
+    plain_geo = float(np.exp(np.mean(np.log(plain_gteps))))
+    # aggregate over ranks (replicas): every rank solved every graph K times
+    value = ws * geo * kern_ms / kern_ms_max
+    aggregate = ws * a.steps * sum(mr) / (kern_ms_max * 1e-3) / 1e9
+    e2e_value = ws * e2e_steps * sum(mr) / (e2e_ms_max * 1e-3) / 1e9
+
+    peak, peak_src = load_peaks()
+    b_alg = [per[sd]["b_alg"] for sd in seeds]
+    achieved = a.steps * sum(b_alg) / (kern_ms * 1e-3) / 1e9
+    traffic = _traffic(wl + ("_learned" if use_learned else ""))
+
+    cpu_line = None
+    if cpu is not None:
+        res = cpu.collect()
+        fn = nps.fnv1a
+        exact = {str(sd): bool(res[sd]["fnv"] == fn(d_head[j]) and res[sd]["fnv"] == fn(d_plain[j]))
+                 for j, sd in enumerate(seeds)}
+        secs = [res[sd]["times"][0] for sd in seeds]
+        use_ref = _cpu_use_ref()
+        cpu_line = {"value": float(np.mean([m / t / 1e9 for m, t in zip(mr, secs)])), "unit": "GTEPS", "cores": 1,
+                    "kind": "reference" if use_ref else "port",
+                    "sample": f"one full SSSP of each of the {len(seeds)} graphs, 1 thread each, "
+                              + ("by the reference's SSSP_CPU (heap Dijkstra, apps/sssp/src/cpu/sssp.cpp, built "
+                                 "from its sources), including its Heap() init" if use_ref else
+                                 "by the oracle's restated heap Dijkstra")
+                              + f"; the {len(seeds)} processes ran at once, beside the GPU timing",
+                    "seconds_per_seed": {str(sd): t for sd, t in zip(seeds, secs)},
+                    "bit_exact_vs_gpu": all(exact.values()), "bit_exact_per_seed": exact}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": ws, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": kern_ms_max / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": rmat_eval_config(wl, desc, seeds, per),
+            "value_definition": "geometric mean over the graphs of m_r * K / (sum of the graph's K CUDA-event "
+                                "SSSP times); aggregate_gteps = all reached edges / all SSSP time",
+            "aggregate_gteps": aggregate,
+            "ms_per_sssp": kern_ms_max / a.steps / len(seeds),
+            "policy": "learned" if use_learned else "plain",
+            "params": dataclasses.asdict(params),
+            "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
+            "tuning": {"graph": f"R-MAT scale {w['scale']} seed {w['tune_seed']} (not an evaluation graph)",
+                       "autotune_evaluations": len(tune_log)},
+            "per_seed": [{"seed": sd, "m_r": per[sd]["m_r"], "ms": seed_ms[j] / a.steps,
+                          "gteps": gteps[j], "plain_ms": plain_seed_ms[j] / a.steps, "plain_gteps": plain_gteps[j],
+                          "iterations": stats[j].iterations, "buckets": stats[j].buckets,
+                          "edges_scanned": stats[j].edges_scanned,
+                          "plain_iterations": plain_stats[j].iterations,
+                          "plain_edges_scanned": plain_stats[j].edges_scanned,
+                          "step_ms_min": min(step_ms[j]), "step_ms_max": max(step_ms[j])}
+                         for j, sd in enumerate(seeds)],
+            "plain": {"value": plain_geo, "unit": "GTEPS", "ms_per_step": plain_ms_max / a.steps,
+                      "params": dataclasses.asdict(plain),
+                      "note": "plain autotuned kernel (fixed parameters, no policy), same graphs, same timing"},
+            "learned_over_plain": (geo / plain_geo) if use_learned else None,
+            "bit_exact": {"learned_vs_plain": exact_vs_plain,
+                          "vs_cpu_dijkstra": cpu_line["bit_exact_vs_gpu"] if cpu_line else None},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                         "traffic_note": "DRAM bytes of one launch on seed 1000 (profiles/traffic.json)",
+                         "b_alg_bytes_per_seed": b_alg, "b_alg_formula": "12*m_r + 12*n_r + 4*n"},
+            "e2e": {"value": e2e_value, "unit": "GTEPS",
+                    "h2d_bytes_per_step": sum(4 * (per[sd]["n"] + 1) + 8 * per[sd]["m"] for sd in seeds),
+                    "d2h_bytes_per_step": sum(4 * per[sd]["n"] for sd in seeds),
+                    "ms_per_step": e2e_ms_max / e2e_steps, "steps": e2e_steps,
+                    "bit_exact_vs_device_run": e2e_ok,
+                    "call": "nps.sssp(host Graph, pinned) once per graph per step"},
+            "gpu_launches": a.steps * len(seeds),
+            "clocks": clocks,
+            "cpu_baseline": cpu_line,
+        }
+        print(json.dumps(line))
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -971,12 +1353,21 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--tune-budget", type=int, default=24, help="autotuner evaluations before timing")
+    ap.add_argument("--seeds", default=None, help="rmat22 only: comma-separated subset of the evaluation seeds")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
+    a.seeds = tuple(int(x) for x in a.seeds.split(",")) if a.seeds else None
 
     ws, rank, local = dist_env()
-    nps = importlib.import_module("nested-parallelism_b200")
     kind, _, desc = WORKLOADS[a.workload]
+    if kind == "rmat_eval":
+        if a.impl == "reference":
+            if rank != 0:
+                return 0
+            print(json.dumps(reference_rmat_eval(a, a.workload, desc)))
+            return 0
+        return bench_rmat_eval(a, ws, rank, local, a.workload, desc)
+    nps = importlib.import_module("nested-parallelism_b200")
     if kind == "batch":
         return bench_batch(a, nps, ws, rank, local, desc)
     if kind == "degree":

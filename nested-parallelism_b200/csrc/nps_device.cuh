@@ -56,7 +56,15 @@ constexpr uint32_t kFull = 0xffffffffu;
 constexpr uint32_t kInf = NPS_INF;
 constexpr int kHeavyShift = 36;  // heavy counter packs (count << 36) | chunk_offset
 constexpr unsigned long long kHeavyMask = (1ull << kHeavyShift) - 1;
-constexpr int kStripes = 8;            // striped work counters
+#ifndef NPS_STRIPES
+#define NPS_STRIPES 8
+#endif
+#ifndef NPS_FLUSH_AT
+#define NPS_FLUSH_AT 64
+#endif
+constexpr int kStripes = NPS_STRIPES;  // striped work counters (at most 32: one per lane when probed)
+static_assert(kStripes >= 1 && kStripes <= 32, "stripes are probed one per lane");
+constexpr uint32_t kStripeMask = kStripes >= 32 ? 0xffffffffu : ((1u << kStripes) - 1u);
 constexpr int kBlockListCap = 512;     // CTA list entries (block tier)
 
 // Per-instance device counters.  Zeroed by the host before a launch.
@@ -436,7 +444,7 @@ __device__ __forceinline__ void append_k(int32_t* q, uint32_t* tail, uint32_t ca
 // in multiples of 32, with one atomicAdd on the queue tail: fewer, larger flushes
 // keep the single tail counter of each queue from serialising the improvements
 // of a large iteration.
-constexpr int kFlushAt = 64;
+constexpr int kFlushAt = NPS_FLUSH_AT;
 constexpr int kStage = kFlushAt + 4 * 32;  // >= kFlushAt - 1 left over + 4 * 32 from one append
 
 struct Stage {
@@ -501,10 +509,18 @@ template <int K>
 __device__ __forceinline__ void relax_and_push(const InstDesc& I, const IterCtx& C, const bool (&valid)[K],
                                                const int32_t (&v)[K], const uint32_t (&nd)[K], Acc& acc,
                                                Stage& S, int lane) {
+  static_assert(K == 4 || K == 8, "candidates per lane");
   bool pn[K], pf[K];
   relax_batch<K>(I, C, valid, v, nd, pn, pf, acc);
-  stage_k<K>(S.nbuf, S.ncnt, pn, v, C.qn, C.qn_tail, I.qcap, &I.ctr->status, lane);
-  stage_k<K>(S.fbuf, S.fcnt, pf, v, C.fp, C.fp_tail, I.qcap, &I.ctr->status, lane);
+  // staged four per lane at a time: a staging buffer holds one such append beyond its flush point
+#pragma unroll
+  for (int h = 0; h < K; h += 4) {
+    const bool fn[4] = {pn[h], pn[h + 1], pn[h + 2], pn[h + 3]};
+    const bool ff[4] = {pf[h], pf[h + 1], pf[h + 2], pf[h + 3]};
+    const int32_t vv[4] = {v[h], v[h + 1], v[h + 2], v[h + 3]};
+    stage_k<4>(S.nbuf, S.ncnt, fn, vv, C.qn, C.qn_tail, I.qcap, &I.ctr->status, lane);
+    stage_k<4>(S.fbuf, S.fcnt, ff, vv, C.fp, C.fp_tail, I.qcap, &I.ctr->status, lane);
+  }
 }
 
 // Load the 16-byte chunk at edge index c (4-aligned) of the column and weight
@@ -895,10 +911,15 @@ __device__ __forceinline__ void walk_chunks(const InstDesc& I, const IterCtx& C,
 // One work item of the grid-tier list L (cnt entries sorted by chunk offset):
 // chunks [kb, ke) of its flat chunk space, whose first chunk lies in entry js.
 // The warp loads 32 consecutive entries at a time (one coalesced load); each
-// lane finds the owner of its chunk among them with a 5-step shuffle search.
+// lane finds the owner of its chunks among them with a 5-step shuffle search.
 // The owners' distances are read at walk time, one per window lane.
 // Every entry has at least one chunk, so a window of 32 entries covers any 32
-// consecutive chunks that start in its first entry.  Warp-collective.
+// consecutive chunks that start in its first entry.
+//
+// A round takes 64 chunks, two per lane (chunks k0 + lane and k0 + 32 + lane):
+// both chunks' column and weight loads are issued together, then their eight
+// distance loads, then their eight atomicMin, so one round costs one dependent
+// chain for 256 edges.  Warp-collective.
 __device__ __forceinline__ void walk_item(const InstDesc& I, const IterCtx& C, const int4* L, uint32_t cnt,
                                           uint32_t kb, uint32_t ke, uint32_t js, Acc& acc, Stage& S, int lane) {
   uint32_t k = kb;
@@ -914,27 +935,49 @@ __device__ __forceinline__ void walk_item(const InstDesc& I, const IterCtx& C, c
       if (v < (uint32_t)I.n) dv = __ldcg(I.dist + v);
     }
     const uint32_t lim = min(ke, __shfl_sync(kFull, cov, 31));  // end of the window's chunks
-    for (uint32_t k0 = k; k0 < lim; k0 += 32) {
-      const uint32_t kk = k0 + lane;
-      const bool act = kk < lim;
-      int o = 0;  // largest window index whose first chunk is <= kk (entry 0's is <= k0)
+    for (uint32_t k0 = k; k0 < lim; k0 += 64) {
+      bool act[2];
+      int32_t s[2], e[2], z[2], c[2];
+      uint32_t du[2];
 #pragma unroll
-      for (int step = 16; step >= 1; step >>= 1) {
-        const uint32_t x = __shfl_sync(kFull, off, o + step);
-        if (x <= kk) o += step;
+      for (int h = 0; h < 2; ++h) {
+        const uint32_t kk = k0 + 32 * h + lane;
+        int o = 0;  // largest window index whose first chunk is <= kk (entry 0's is <= k0)
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1) {
+          const uint32_t x = __shfl_sync(kFull, off, o + step);
+          if (x <= kk) o += step;
+        }
+        s[h] = __shfl_sync(kFull, E.x, o);
+        e[h] = __shfl_sync(kFull, E.y, o);
+        z[h] = __shfl_sync(kFull, E.z, o);
+        du[h] = __shfl_sync(kFull, dv, o);
+        const uint32_t oo = __shfl_sync(kFull, off, o);
+        // the owner must hold chunk kk (it always does unless the list is inconsistent)
+        const bool own = kk >= oo && e[h] > s[h] && kk - oo < row_chunks(s[h], e[h]);
+        if (kk < lim && !own) atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_CAPACITY);
+        act[h] = kk < lim && own;
+        c[h] = (s[h] & ~3) + 4 * (int32_t)(kk - oo);
       }
-      const int32_t s = __shfl_sync(kFull, E.x, o);
-      const int32_t e = __shfl_sync(kFull, E.y, o);
-      const int32_t z = __shfl_sync(kFull, E.z, o);
-      const uint32_t du = __shfl_sync(kFull, dv, o);
-      const uint32_t oo = __shfl_sync(kFull, off, o);
-      // the owner must hold chunk kk (it always does unless the list is inconsistent)
-      const bool own = kk >= oo && e > s && kk - oo < row_chunks(s, e);
-      if (act && !own) atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_CAPACITY);
-      const int32_t c = (s & ~3) + 4 * (int32_t)(kk - oo);
-      int4 cv, wv;
-      load_chunk(I, act && own, c, s, e, cv, wv);
-      relax_loaded(I, C, act && own, c, s, e, du, z < 0, cv, wv, acc, S, lane);
+      int4 cv[2], wv[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) load_chunk(I, act[h], c[h], s[h], e[h], cv[h], wv[h]);
+      bool valid[8];
+      int32_t v[8];
+      uint32_t nd[8];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int32_t cc[4] = {cv[h].x, cv[h].y, cv[h].z, cv[h].w};
+        const uint32_t ww[4] = {(uint32_t)wv[h].x, (uint32_t)wv[h].y, (uint32_t)wv[h].z, (uint32_t)wv[h].w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int32_t ei = c[h] + q;
+          valid[4 * h + q] = act[h] && ei >= s[h] && ei < e[h] && edge_in_pass(C, ww[q], z[h] < 0);
+          v[4 * h + q] = cc[q];
+          nd[4 * h + q] = tent(du[h], ww[q]);
+        }
+      }
+      relax_and_push<8>(I, C, valid, v, nd, acc, S, lane);
     }
     k = lim;
     js += 32;
@@ -1193,7 +1236,8 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
             const bool avail = lane < kStripes && ld_relaxed_u32(&wc[lane * 32]) < li;
             const uint32_t m = __ballot_sync(kFull, avail);
             if (m == 0) break;
-            const uint32_t rot = ((m >> (stripe + 1)) | (m << (kStripes - stripe - 1))) & ((1u << kStripes) - 1);
+            const unsigned long long mm = (unsigned long long)m | ((unsigned long long)m << kStripes);
+            const uint32_t rot = (uint32_t)(mm >> (stripe + 1)) & kStripeMask;  // m rotated right by stripe + 1
             stripe = (stripe + __ffs(rot)) % kStripes;
             continue;
           }

@@ -58,8 +58,29 @@ def _load_oracle():
         lib.oracle_color.restype = _I32
         lib.oracle_color_iterations.argtypes = [_I32, _P, _P, _P]
         lib.oracle_color_iterations.restype = _I32
+        lib.oracle_gen_rmat.argtypes = [_I32, _I32, _D, _D, _D, C.c_uint32, C.c_uint64, _P, _P, _P,
+                                        C.POINTER(_I32)]
+        lib.oracle_gen_rmat.restype = _I64
         _orc = lib
     return _orc
+
+
+def gen_rmat(scale: int, edge_factor: int = 16, seed: int = 1, a: float = 0.57, b: float = 0.19,
+             c: float = 0.19, wmax: int = 255):
+    """The benchmark's seeded R-MAT graph (deduplicated, no self-loops, rows in reverse
+    edge order), identical to the library's gen_rmat.  Returns (row_ptr int32[n+1],
+    col int32[m], w uint32[m], source)."""
+    lib = _load_oracle()
+    n, m = 1 << scale, edge_factor << scale
+    row = np.empty(n + 1, dtype=np.int32)
+    col = np.empty(m, dtype=np.int32)
+    w = np.empty(m, dtype=np.uint32)
+    src = _I32(0)
+    k = lib.oracle_gen_rmat(scale, edge_factor, a, b, c, wmax, seed, row.ctypes.data, col.ctypes.data,
+                            w.ctypes.data, C.byref(src))
+    if k < 0:
+        raise ValueError("gen_rmat: bad parameters")
+    return row, col[:k].copy(), w[:k].copy(), int(src.value)
 
 
 def have_reference() -> bool:

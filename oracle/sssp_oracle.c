@@ -46,6 +46,10 @@
  *                      those are final when v is reached.  The reference has no CPU
  *                      version of this path (parity unpinned: see the test header).
  *
+ *   oracle_gen_rmat    the benchmark's seeded R-MAT input (a restatement of this
+ *                      library's own generator, so the reference's CPU path can be
+ *                      timed on the same graph without loading the library).
+ *
  * Distances are uint32 with INF = 2^30 (sssp_wrapper.cu:7, common/global.h:19).
  * A tentative distance that reaches 2^30 is treated as unreachable; the
  * reference's int arithmetic never gets there on the inputs it is run on.
@@ -405,4 +409,104 @@ int32_t oracle_color_iterations(int32_t n, const int32_t* row, const int32_t* co
     }
   }
   return c;
+}
+
+/* ------------------------------------------------------------------------
+ * oracle_gen_rmat: the seeded R-MAT input of the benchmark, restated in C so
+ * that the reference's CPU path can be run on the very same graph without
+ * loading the library under test.  It follows nps_gen_rmat and nps_build_csr
+ * (nested-parallelism_b200/csrc/nps_graph.cpp): edge e draws from the counter
+ * stream key = splitmix64(splitmix64(seed ^ salt) ^ e * 0xD6E8FEB86659FD93),
+ * draw k = splitmix64(key + k * 0x9E3779B97F4A7C15); `scale` quadrant draws
+ * (53-bit uniforms, most significant level first), then the weight
+ * 1 + ((draw >> 32) * wmax >> 32).  Self-loops are dropped, duplicate
+ * (src, dst) pairs keep their earliest edge, rows hold their edges in reverse
+ * edge order (the reference's convertCSR convention), and the source is the
+ * highest out-degree vertex (lowest id on ties).  The edge draws run on the
+ * host's threads; the CSR is built in one O(m) pass: rows are filled in
+ * ascending edge order and a per-destination stamp drops repeats.
+ * Caller passes row[n+1], col[m], w[m] with m = edge_factor << scale; returns the
+ * kept edge count (or -1 on a bad argument) and the source in *src_out.
+ */
+static uint64_t sm64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+int64_t oracle_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c, uint32_t wmax,
+                        uint64_t seed, int32_t* row, int32_t* col, uint32_t* w, int32_t* src_out) {
+  if (scale < 1 || scale > 30 || edge_factor < 1 || wmax == 0) return -1;
+  const int64_t n = (int64_t)1 << scale, m = n * edge_factor;
+  const double ab = a + b, abc = a + b + c;
+  const uint64_t salt = 0x726D617431323334ull;
+  int32_t* es = (int32_t*)malloc(sizeof(int32_t) * (size_t)m);
+  int32_t* ed = (int32_t*)malloc(sizeof(int32_t) * (size_t)m);
+  uint32_t* ew = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)m);
+  int64_t* start = (int64_t*)calloc((size_t)n + 1, sizeof(int64_t));
+  int64_t* fill = (int64_t*)malloc(sizeof(int64_t) * (size_t)n);
+  int64_t* ids = (int64_t*)malloc(sizeof(int64_t) * (size_t)m);
+  int32_t* stamp = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
+  if (!es || !ed || !ew || !start || !fill || !ids || !stamp) {
+    free(es); free(ed); free(ew); free(start); free(fill); free(ids); free(stamp);
+    return -1;
+  }
+  const uint64_t base = sm64(seed ^ salt);
+#pragma omp parallel for schedule(static)
+  for (int64_t e = 0; e < m; ++e) {
+    const uint64_t key = sm64(base ^ ((uint64_t)e * 0xD6E8FEB86659FD93ull));
+    uint64_t k = 0;
+    uint32_t u = 0, v = 0;
+    for (int l = scale - 1; l >= 0; --l) {
+      const double x = (double)(sm64(key + (k++) * 0x9E3779B97F4A7C15ull) >> 11) * (1.0 / 9007199254740992.0);
+      if (x < a) {
+      } else if (x < ab) {
+        v |= 1u << l;
+      } else if (x < abc) {
+        u |= 1u << l;
+      } else {
+        u |= 1u << l;
+        v |= 1u << l;
+      }
+    }
+    es[e] = (int32_t)u;
+    ed[e] = (int32_t)v;
+    ew[e] = 1u + (uint32_t)(((sm64(key + (k++) * 0x9E3779B97F4A7C15ull) >> 32) * (uint64_t)wmax) >> 32);
+  }
+  /* bucket edge ids by source, ascending id within a row */
+  for (int64_t e = 0; e < m; ++e)
+    if (es[e] != ed[e]) start[es[e] + 1]++;
+  for (int64_t v = 0; v < n; ++v) start[v + 1] += start[v];
+  for (int64_t v = 0; v < n; ++v) fill[v] = start[v];
+  for (int64_t e = 0; e < m; ++e)
+    if (es[e] != ed[e]) ids[fill[es[e]]++] = e;
+  /* per row: keep the first edge to each destination, then write the row reversed */
+  for (int64_t v = 0; v < n; ++v) stamp[v] = -1;
+  int64_t o = 0;
+  int32_t best = 0, bestd = -1;
+  for (int64_t v = 0; v < n; ++v) {
+    row[v] = (int32_t)o;
+    int64_t k = 0;
+    for (int64_t i = start[v]; i < start[v + 1]; ++i) {
+      const int32_t d = ed[ids[i]];
+      if (stamp[d] == (int32_t)v) continue;
+      stamp[d] = (int32_t)v;
+      ids[start[v] + k++] = ids[i];
+    }
+    for (int64_t i = 0; i < k; ++i) {
+      const int64_t e = ids[start[v] + k - 1 - i];
+      col[o + i] = ed[e];
+      w[o + i] = ew[e];
+    }
+    if ((int32_t)k > bestd) {
+      bestd = (int32_t)k;
+      best = (int32_t)v;
+    }
+    o += k;
+  }
+  row[n] = (int32_t)o;
+  *src_out = best;
+  free(es); free(ed); free(ew); free(start); free(fill); free(ids); free(stamp);
+  return o;
 }

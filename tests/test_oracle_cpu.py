@@ -101,3 +101,15 @@ def test_restatement_against_the_reference_itself(nps, oracle, seed):
     assert np.array_equal(rd, ref)
     u1, _ = oracle.ref_usssp_cpu(g.row_ptr, g.col, g.w, src, threads=1)  # exact with one thread
     assert np.array_equal(u1, ref)
+
+
+@pytest.mark.parametrize("scale,ef,seed,probs", [(8, 4, 1, (0.57, 0.19, 0.19)), (12, 16, 1000, (0.57, 0.19, 0.19)),
+                                                  (14, 8, 7, (0.45, 0.15, 0.15)), (17, 16, 3, (0.57, 0.19, 0.19))])
+def test_oracle_rmat_input_equals_the_library_generator(nps, oracle, scale, ef, seed, probs):
+    """The benchmark's reference arm builds its input with the oracle's generator (so it
+    never loads the library); it must be the same graph, source included."""
+    a, b, c = probs
+    row, col, w, src = oracle.gen_rmat(scale, ef, seed, a, b, c, 255)
+    g = nps.gen_rmat(scale, ef, a, b, c, seed=seed)
+    assert np.array_equal(row, g.row_ptr) and np.array_equal(col, g.col) and np.array_equal(w, g.w)
+    assert src == g.source
