@@ -113,12 +113,24 @@ typedef struct nps_params {
   uint32_t delta_schedule;  /* 0: every bucket is delta wide.  Otherwise bucket b (0 = the first)
                                is 2^k wide with k = bits [4b, 4b+4) for b < 7 and bits [28, 32)
                                for every later bucket; delta is then unused (plain policy only) */
-  int32_t reserved[3];      /* reserved[0] = 1: test hook, the first in-kernel barrier (of the SSSP
+  int32_t reserved[2];      /* reserved[0] = 1: test hook, the first in-kernel barrier (of the SSSP
                                kernel, or of nps_color's round kernel) waits for an arrival that
                                never comes, so its bounded wait must expire.
                                reserved[1] > 0: nps_bc folds at most this many sources per block
                                of dependency rows (0 = as many as 2 GB of rows hold) */
+  int32_t schedule;         /* NPS_SCHEDULE_* (default NPS_SCHEDULE_ITERATIONS) */
 } nps_params;
+
+/* How the persistent SSSP kernel moves from one frontier to the next. */
+enum {
+  NPS_SCHEDULE_ITERATIONS = 0,  /* frontier iterations separated by a team barrier (every level, batches) */
+  NPS_SCHEDULE_ASYNC = 1        /* single-instance calls at NPS_LEVEL_GRID without light/heavy split or
+                                   local rounds: inside a bucket, improved vertices and 256-edge segments
+                                   of rows of >= threshold edges go to device work rings that every warp
+                                   drains as work appears; the team meets only at bucket advances.  The
+                                   learned policy then picks a width at each advance (stats = iterations
+                                   = buckets); other parameter sets run the iteration schedule */
+};
 
 typedef struct nps_stats {
   uint32_t iterations;      /* frontier iterations (the reference's `iteration` global) */
@@ -240,8 +252,8 @@ nps_status nps_trace_read(int32_t device, nps_trace_rec* out, int32_t cap, int32
  * Limit: n <= NPS_NOALLOC_MAX_VERTICES (larger graphs get NPS_ERR_CAPACITY).
  * The call synchronises its stream to return a status, so it cannot run on a
  * stream being captured into a CUDA graph (NPS_ERR_INVALID_ARG there).  The
- * first call on a device resolves the array's address and caches it; a
- * cudaDeviceReset() of that device invalidates the cached address.  Calls share
+ * first call on a device resolves the array's address and caches it (again after
+ * a cudaDeviceReset() of that device).  Calls share
  * the array: calls whose kernels overlap on the GPU race, so order them on one
  * stream.  No trace, no kernel_ms in the stats.
  * Device pointers only; p->stream selects the stream (NULL = legacy default). */

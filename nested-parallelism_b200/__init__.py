@@ -31,6 +31,7 @@ INF = NPS_INF
 THRESHOLD = 64
 CONSOLIDATE_WARP, CONSOLIDATE_BLOCK, CONSOLIDATE_GRID, CONSOLIDATE_HYBRID = 0, 1, 2, 3
 POLICY_PLAIN, POLICY_LEARNED = 0, 1
+SCHEDULE_ITERATIONS, SCHEDULE_ASYNC = 0, 1
 # `-s <solution>` of the reference CLI (apps/sssp/src/gpu/sssp.cpp:38), the cases of
 # SSSP_GPU()'s switch (apps/sssp/src/gpu/sssp_wrapper.cu:554-566)
 (SOLUTION_TQUEUE, SOLUTION_DUAL_QUEUE, SOLUTION_SHARED_DELAYED, SOLUTION_GLOBAL_DELAYED,
@@ -41,7 +42,7 @@ SOLUTION_NAMES = ("sssp_tqueue_gpu", "sssp_dual_queue_gpu", "sssp_shared_delayed
 
 __all__ = [
     "INF", "THRESHOLD", "CONSOLIDATE_WARP", "CONSOLIDATE_BLOCK", "CONSOLIDATE_GRID",
-    "CONSOLIDATE_HYBRID", "POLICY_PLAIN", "POLICY_LEARNED", "Graph", "Params", "Stats",
+    "CONSOLIDATE_HYBRID", "POLICY_PLAIN", "POLICY_LEARNED", "SCHEDULE_ITERATIONS", "SCHEDULE_ASYNC", "Graph", "Params", "Stats",
     "NpsError", "gen_uniform", "gen_rmat", "gen_grid", "convertCSR", "readInputDIMACS9",
     "readInputDIMACS10", "readInputSLNDC", "writeDIMACS9", "sssp", "sssp_device", "SSSP_GPU",
     "sssp_np_consolidate_gpu", "sssp_solution", "sssp_solution_state", "SolutionInfo",
@@ -221,6 +222,7 @@ class Params:
     delta_schedule: int = 0             # per-bucket log2 widths, 4 bits each (see delta_schedule())
     fault_inject_wait: bool = False     # test hook: the first barrier can never complete
     bc_block_sources: int = 0           # bc: sources per block of dependency rows (0 = as memory allows)
+    schedule: int = 0                   # SCHEDULE_ITERATIONS or SCHEDULE_ASYNC (see include/nps.h)
 
     def to_c(self, device_ptrs: bool, stream: Optional[int] = None) -> nps_params:
         p = nps_params()
@@ -238,6 +240,7 @@ class Params:
         p.stream = stream
         p.reserved[0] = int(bool(self.fault_inject_wait))
         p.reserved[1] = int(self.bc_block_sources)
+        p.schedule = int(self.schedule)
         return p
 
 

@@ -35,7 +35,8 @@ class nps_params(C.Structure):
         ("delta", C.c_uint32), ("policy", C.c_int32), ("device_ptrs", C.c_int32),
         ("device", C.c_int32), ("stream", C.c_void_p), ("timeout_s", C.c_double),
         ("trace", C.c_int32), ("light_heavy", C.c_int32), ("local_rounds", C.c_int32),
-        ("order_degree", C.c_int32), ("delta_schedule", C.c_uint32), ("reserved", C.c_int32 * 3),
+        ("order_degree", C.c_int32), ("delta_schedule", C.c_uint32), ("reserved", C.c_int32 * 2),
+        ("schedule", C.c_int32),
     ]
 
 

@@ -218,6 +218,7 @@ __global__ void bc_check_sources_kernel(const int32_t* sources, int32_t nsrc, in
 
 
 struct BcWork {
+  unsigned long long ctx_id = 0;  // context the cached buffers live in (nps_context_id)
   std::mutex mu;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[4] = {};
@@ -271,7 +272,14 @@ extern "C" nps_status nps_bc(const int32_t* row_ptr, const int32_t* col, int32_t
   {
     std::lock_guard<std::mutex> lk(g_bc_mu);
     if ((int)g_bc.size() <= p.device) g_bc.resize(p.device + 1, nullptr);
-    if (!g_bc[p.device]) g_bc[p.device] = new BcWork();
+    {
+    const unsigned long long id = nps_context_id(p.device);
+    if (g_bc[p.device] && id != 0 && g_bc[p.device]->ctx_id != id) g_bc[p.device] = nullptr;  // device reset: abandoned
+    if (!g_bc[p.device]) {
+      g_bc[p.device] = new BcWork();
+      g_bc[p.device]->ctx_id = id;
+    }
+  }
     W = g_bc[p.device];
   }
   std::lock_guard<std::mutex> lk(W->mu);

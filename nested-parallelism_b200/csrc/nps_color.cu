@@ -456,6 +456,7 @@ __global__ void color_left_kernel(const int32_t* color, int32_t n, uint32_t* lef
 
 
 struct ColorWork {
+  unsigned long long ctx_id = 0;  // context the cached buffers live in (nps_context_id)
   std::mutex mu;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[4] = {};
@@ -509,7 +510,14 @@ extern "C" nps_status nps_color(const int32_t* row_ptr, const int32_t* col, int3
   {
     std::lock_guard<std::mutex> lk(g_color_mu);
     if ((int)g_color.size() <= p.device) g_color.resize(p.device + 1, nullptr);
-    if (!g_color[p.device]) g_color[p.device] = new ColorWork();
+    {
+    const unsigned long long id = nps_context_id(p.device);
+    if (g_color[p.device] && id != 0 && g_color[p.device]->ctx_id != id) g_color[p.device] = nullptr;  // device reset: abandoned
+    if (!g_color[p.device]) {
+      g_color[p.device] = new ColorWork();
+      g_color[p.device]->ctx_id = id;
+    }
+  }
     W = g_color[p.device];
   }
   std::lock_guard<std::mutex> lk(W->mu);

@@ -128,6 +128,7 @@ __global__ void __launch_bounds__(kThreads) degree_pass2(const int32_t* __restri
 // Per-device cached buffers: the staged row_ptr (host-pointer calls), the
 // accumulators and the distribution.
 struct DegWork {
+  unsigned long long ctx_id = 0;  // context the cached buffers live in (nps_context_id)
   int32_t* rp = nullptr;
   size_t rp_n = 0;
   DegAcc* acc = nullptr;
@@ -143,7 +144,14 @@ std::vector<DegWork*> g_deg;
 DegWork* deg_work(int device) {
   std::lock_guard<std::mutex> lk(g_deg_mu);
   if ((int)g_deg.size() <= device) g_deg.resize(device + 1, nullptr);
-  if (!g_deg[device]) g_deg[device] = new DegWork();
+  {
+    const unsigned long long id = nps_context_id(device);
+    if (g_deg[device] && id != 0 && g_deg[device]->ctx_id != id) g_deg[device] = nullptr;  // device reset: abandoned
+    if (!g_deg[device]) {
+      g_deg[device] = new DegWork();
+      g_deg[device]->ctx_id = id;
+    }
+  }
   return g_deg[device];
 }
 

@@ -90,9 +90,23 @@ struct __align__(128) Counters {
   uint32_t pad1[3];
   unsigned long long prof[9];   // NPS_PROFILE builds: SM cycles per phase, summed over warps
   unsigned long long solve_ns;  // end of this instance's solve, from its team CTA 0's start
-  unsigned long long pad2[6];
+  // asynchronous buckets: ring units (near-ring vertices and segments) pushed and not yet
+  // processed, and the phase's static items claimed and done, slot = phase % 3
+  uint32_t pend;
+  uint32_t swork[3];
+  uint32_t sdone[3];
+  uint32_t pad2[5];
   // striped work counters, one 128-byte line each: work[slot][stripe * 32]
   uint32_t work[3][kStripes * 32];
+};
+
+// Work rings of the asynchronous buckets.  Head and tail counters persist across
+// runs on a workspace (like the stamp base), each on its own 128-byte line.
+struct __align__(128) RingState {
+  uint32_t nq_head, pad0[31];
+  uint32_t nq_tail, pad1[31];
+  uint32_t seg_head, pad2[31];
+  uint32_t seg_tail, pad3[31];
 };
 
 struct InstDesc {
@@ -130,6 +144,13 @@ struct InstDesc {
   int32_t local_rounds; // warp-local processing rounds per vertex item (0 = none)
   int32_t order_degree; // rows below this degree ignore the bucket bound (0 = none)
   uint32_t dsched;      // per-bucket log2 widths, 4 bits each (0 = fixed delta)
+  int32_t async;        // 1: buckets are processed without per-iteration barriers (GRID tiers)
+  unsigned long long* nq;  // near ring: slot = (tag << 32) | vertex, tag = index + 1 when filled
+  uint32_t nq_mask;        // ring capacity - 1 (a power of two)
+  int4* seg;               // segment ring: {start, end, vertex | heavy flag, tag}
+  uint32_t seg_mask;
+  RingState* rs;
+  unsigned long long wait_ns;  // bound on one wait for a ring slot
 };
 
 struct TeamDesc {
@@ -188,6 +209,33 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
   unsigned long long v;
   asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
+}
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64p(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ void st_relaxed_u32(uint32_t* p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void st_release_u32(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Zero that the compiler cannot see through: adding it to an address makes a
+// later access wait for the value it was made from (a data dependency, so the
+// access is issued only after that value has returned from memory).
+__device__ __forceinline__ uint32_t dep_zero(uint32_t x) {
+  uint32_t z;
+  asm volatile("and.b32 %0, %1, 0;" : "=r"(z) : "r"(x));
+  return z;
 }
 
 // L2 cache policies (createpolicy, sm_80+): the CSR column/weight stream is
@@ -304,6 +352,8 @@ struct IterCtx {
   uint32_t sstamp;
   int32_t local_rounds;  // rounds of warp-local processing per vertex item
   int32_t order_deg;     // improved vertices below this degree join the near queue at any distance
+  bool ring;             // asynchronous bucket: near pushes go to the near ring, grid-tier rows
+                         // to the segment ring (qn, heavy and the item tables are unused)
 };
 
 // Whether an edge of weight w is relaxed by a pass over light (heavy = false)
@@ -388,6 +438,8 @@ __device__ __forceinline__ void relax_batch(const InstDesc& I, const IterCtx& C,
       bool near = nd[j] < C.T;
       if (!near && C.order_deg > 0) near = __ldg(I.row_ptr + v[j] + 1) - __ldg(I.row_ptr + v[j]) < C.order_deg;
       if (near) {
+        // (ring mode: the exchange is issued only once this atomicMin has returned, so a
+        // consumer that sees the mark set sees the new distance too)
         pn[j] = atomicExch(I.mark + v[j], C.snear) != C.snear;
       } else {
         pf[j] = atomicExch(I.fmark + v[j], C.sfar) != C.sfar;
@@ -454,6 +506,8 @@ struct Stage {
   uint32_t ncnt;   // warp-uniform fill counts
   uint32_t fcnt;
   uint32_t scnt;
+  uint32_t fmin;   // per lane: smallest distance pushed into the far pile (ring mode)
+  uint32_t* credit;  // ring mode: pending-total credits this warp holds (shared memory, lane 0)
 };
 
 // Move the first `nflush` staged entries to q and shift the rest down.
@@ -476,9 +530,73 @@ __device__ __forceinline__ void stage_flush(int32_t* buf, uint32_t& cnt, uint32_
   cnt = rem;
 }
 
+// Wait (bounded by I.wait_ns) until the previous user of a ring slot has released it,
+// i.e. its tag equals `want`.  False, with NPS_ERR_TIMEOUT recorded, when the bound
+// runs out or another error already stopped the run.
+static __device__ __noinline__ bool ring_wait_tag(const uint32_t* tag, uint32_t want, const InstDesc& I) {
+  const unsigned long long t0 = globaltimer_ns();
+  for (;;) {
+    if (ld_relaxed_u32(tag) == want) return true;
+    if (ld_relaxed_u32(&I.ctr->status) != 0) return false;
+    if (globaltimer_ns() - t0 > I.wait_ns) {
+      atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_TIMEOUT);
+      return false;
+    }
+    __nanosleep(64);
+  }
+}
+
+// Ring mode: units this warp makes visible are first covered by credits it holds
+// in the pending total.  Lane 0 takes `k` credits, adding a batch of at least
+// kCreditBatch to the pending total when its own run out (one atomic per batch,
+// not per flush); the returned value orders the addition before anything made
+// visible from it (callers add dep_zero of the result to their next address).
+constexpr uint32_t kCreditBatch = 1024;
+__device__ __forceinline__ uint32_t take_credits(const InstDesc& I, uint32_t* credit, uint32_t k) {
+  uint32_t c = *credit, x = 0;
+  if (c < k) {
+    const uint32_t add = max(k - c, kCreditBatch);
+    x = atomicAdd(&I.ctr->pend, add);
+    c += add;
+  }
+  *credit = c - k;
+  return x;
+}
+
+// Move the first `nflush` staged entries to the near ring and shift the rest down.
+// The entries are covered by pending-total credits before they become visible (the
+// ring reservation waits for the credits), so the total cannot reach zero while one
+// of them waits or is being processed.  Slot = (index + 1) << 32 | vertex, one
+// 8-byte store, written once its previous user released it (tag == index).
+__device__ __forceinline__ void ring_flush(const InstDesc& I, int32_t* buf, uint32_t& cnt, uint32_t nflush,
+                                           int lane, uint32_t* credit) {
+  __syncwarp();
+  uint32_t base = 0;
+  if (lane == 0) {
+    const uint32_t x = take_credits(I, credit, nflush);
+    base = atomicAdd(&I.rs->nq_tail + dep_zero(x), nflush);
+  }
+  base = __shfl_sync(kFull, base, 0);
+  for (uint32_t i = lane; i < nflush; i += 32) {
+    const uint32_t idx = base + i;
+    unsigned long long* slot = I.nq + (idx & I.nq_mask);
+    const uint32_t* tag = reinterpret_cast<const uint32_t*>(slot) + 1;  // high word (little-endian)
+    if (ld_relaxed_u32(tag) == idx || ring_wait_tag(tag, idx, I))
+      st_relaxed_u64(slot, ((unsigned long long)(idx + 1) << 32) | (uint32_t)buf[i]);
+  }
+  const uint32_t rem = cnt - nflush;
+  int32_t t = 0;
+  if ((uint32_t)lane < rem) t = buf[nflush + lane];
+  __syncwarp();
+  if ((uint32_t)lane < rem) buf[lane] = t;
+  __syncwarp();
+  cnt = rem;
+}
+
 template <int K>
 __device__ __forceinline__ void stage_k(int32_t* buf, uint32_t& cnt, const bool (&f)[K], const int32_t (&v)[K],
-                                        int32_t* q, uint32_t* tail, uint32_t cap, uint32_t* status, int lane) {
+                                        int32_t* q, uint32_t* tail, uint32_t cap, uint32_t* status, int lane,
+                                        const InstDesc* ring = nullptr, uint32_t* credit = nullptr) {
   uint32_t b[K];
   uint32_t tot = 0;
 #pragma unroll
@@ -495,12 +613,20 @@ __device__ __forceinline__ void stage_k(int32_t* buf, uint32_t& cnt, const bool 
     base += __popc(b[j]);
   }
   cnt += tot;
-  if (cnt >= (uint32_t)kFlushAt) stage_flush(buf, cnt, cnt & ~31u, q, tail, cap, status, lane);
+  if (cnt >= (uint32_t)kFlushAt) {
+    if (ring) ring_flush(*ring, buf, cnt, cnt & ~31u, lane, credit);
+    else stage_flush(buf, cnt, cnt & ~31u, q, tail, cap, status, lane);
+  }
 }
 
-// End of an iteration: everything staged goes to the global queues.
-__device__ __forceinline__ void stage_drain(Stage& S, const IterCtx& C, uint32_t qcap, uint32_t* status, int lane) {
-  if (S.ncnt) stage_flush(S.nbuf, S.ncnt, S.ncnt, C.qn, C.qn_tail, qcap, status, lane);
+// End of an iteration: everything staged goes to the global queues (near pushes to
+// the near ring in ring mode).
+__device__ __forceinline__ void stage_drain(const InstDesc& I, Stage& S, const IterCtx& C, uint32_t qcap,
+                                            uint32_t* status, int lane) {
+  if (S.ncnt) {
+    if (C.ring) ring_flush(I, S.nbuf, S.ncnt, S.ncnt, lane, S.credit);
+    else stage_flush(S.nbuf, S.ncnt, S.ncnt, C.qn, C.qn_tail, qcap, status, lane);
+  }
   if (S.fcnt) stage_flush(S.fbuf, S.fcnt, S.fcnt, C.fp, C.fp_tail, qcap, status, lane);
   if (S.scnt) stage_flush(S.sbuf, S.scnt, S.scnt, C.sq, C.sq_tail, qcap, status, lane);
 }
@@ -518,8 +644,14 @@ __device__ __forceinline__ void relax_and_push(const InstDesc& I, const IterCtx&
     const bool fn[4] = {pn[h], pn[h + 1], pn[h + 2], pn[h + 3]};
     const bool ff[4] = {pf[h], pf[h + 1], pf[h + 2], pf[h + 3]};
     const int32_t vv[4] = {v[h], v[h + 1], v[h + 2], v[h + 3]};
-    stage_k<4>(S.nbuf, S.ncnt, fn, vv, C.qn, C.qn_tail, I.qcap, &I.ctr->status, lane);
+    stage_k<4>(S.nbuf, S.ncnt, fn, vv, C.qn, C.qn_tail, I.qcap, &I.ctr->status, lane, C.ring ? &I : nullptr,
+               S.credit);
     stage_k<4>(S.fbuf, S.fcnt, ff, vv, C.fp, C.fp_tail, I.qcap, &I.ctr->status, lane);
+  }
+  if (C.ring) {
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+      if (pf[j]) S.fmin = min(S.fmin, nd[j]);
   }
 }
 
@@ -573,6 +705,7 @@ struct Smem {
   float feat[NPS_MLP_IN];
   int32_t pol_choice[2];
   uint32_t it_acc[3];          // this CTA's edges, improvements, first reaches in the iteration
+  uint32_t credit[BS / 32];    // ring mode: pending-total credits held per warp
   TeamDesc team;
   int32_t team_id;
   uint32_t rank;
@@ -684,6 +817,109 @@ __device__ __forceinline__ void warp_row(const InstDesc& I, const IterCtx& C, in
   }
 }
 
+// Ring mode: the grid-tier rows of a warp become segments of at most 256 edges
+// (64 chunks from the row's 4-aligned start) on the segment ring.  The segments
+// are covered by pending-total credits before they are visible; one reservation
+// per warp.
+// Returns false, pushing nothing, when the ring is more than half full: the rows
+// are then walked by the warp itself.  Warp-collective.
+__device__ __forceinline__ bool push_segments(const InstDesc& I, bool gtier, int32_t s, int32_t e, int32_t vtag,
+                                              int lane, uint32_t* credit) {
+  const uint32_t nseg = gtier ? (uint32_t)(((int64_t)e - (s & ~3) + 255) >> 8) : 0u;
+  uint32_t incl = nseg;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const uint32_t total = __shfl_sync(kFull, incl, 31);
+  if (total == 0) return true;
+  uint32_t base = 0, ok = 1;
+  if (lane == 0) {
+    const int32_t used = (int32_t)(ld_relaxed_u32(&I.rs->seg_tail) - ld_relaxed_u32(&I.rs->seg_head));
+    if ((int64_t)max(used, 0) + total > (int64_t)(I.seg_mask + 1) / 2) {
+      ok = 0;
+    } else {
+      const uint32_t x = take_credits(I, credit, total);
+      base = atomicAdd(&I.rs->seg_tail + dep_zero(x), total);
+    }
+  }
+  if (!__shfl_sync(kFull, ok, 0)) return false;
+  base = __shfl_sync(kFull, base, 0);
+  const uint32_t excl = incl - nseg;
+  uint32_t wb = __ballot_sync(kFull, nseg > 0);
+  while (wb) {
+    const int src = __ffs(wb) - 1;
+    wb &= wb - 1;
+    const int32_t rs = __shfl_sync(kFull, s, src), re = __shfl_sync(kFull, e, src);
+    const int32_t rz = __shfl_sync(kFull, vtag, src);
+    const uint32_t rn = __shfl_sync(kFull, nseg, src), rx = __shfl_sync(kFull, excl, src);
+    const int64_t c0 = rs & ~3;
+    for (uint32_t j = lane; j < rn; j += 32) {
+      const uint32_t idx = base + rx + j;
+      int4* slot = I.seg + (idx & I.seg_mask);
+      uint32_t* tag = reinterpret_cast<uint32_t*>(slot) + 3;
+      if (ld_relaxed_u32(tag) == idx || ring_wait_tag(tag, idx, I)) {
+        int32_t* w = reinterpret_cast<int32_t*>(slot);
+        w[0] = (int32_t)max((int64_t)rs, c0 + 256 * (int64_t)j);
+        w[1] = (int32_t)min((int64_t)re, c0 + 256 * ((int64_t)j + 1));
+        w[2] = rz;
+      }
+    }
+  }
+  // every payload is in place before any tag says so: one fence, then the tags
+  __threadfence();
+  wb = __ballot_sync(kFull, nseg > 0);
+  while (wb) {
+    const int src = __ffs(wb) - 1;
+    wb &= wb - 1;
+    const uint32_t rn = __shfl_sync(kFull, nseg, src), rx = __shfl_sync(kFull, excl, src);
+    for (uint32_t j = lane; j < rn; j += 32) {
+      const uint32_t idx = base + rx + j;
+      uint32_t* tag = reinterpret_cast<uint32_t*>(I.seg + (idx & I.seg_mask)) + 3;
+      if (ld_relaxed_u32(&I.ctr->status) == 0) st_relaxed_u32(tag, idx + 1);
+    }
+  }
+  return true;
+}
+
+// One segment {start, end, vertex | heavy flag} of at most 256 edges starting at a
+// 4-aligned chunk: two chunks per lane, one batch of eight candidates.  The owner's
+// distance is read now (it may have dropped since the segment was pushed; the owner
+// is then queued again for the drop).  Warp-collective.
+__device__ __forceinline__ void walk_segment(const InstDesc& I, const IterCtx& C, int4 sg, Acc& acc, Stage& S,
+                                             int lane) {
+  const int32_t s = sg.x, e = sg.y;
+  const uint32_t v = (uint32_t)sg.z & 0x7fffffffu;
+  const uint32_t du = v < (uint32_t)I.n ? __ldcg(I.dist + v) : kInf;
+  const int32_t c0 = s & ~3;
+  bool act[2];
+  int32_t c[2];
+  int4 cv[2], wv[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    c[h] = c0 + 128 * h + 4 * lane;
+    act[h] = s >= 0 && e <= I.m && c[h] < e;
+    load_chunk(I, act[h], c[h], s, e, cv[h], wv[h]);
+  }
+  bool valid[8];
+  int32_t vv[8];
+  uint32_t nd[8];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int32_t cc[4] = {cv[h].x, cv[h].y, cv[h].z, cv[h].w};
+    const uint32_t ww[4] = {(uint32_t)wv[h].x, (uint32_t)wv[h].y, (uint32_t)wv[h].z, (uint32_t)wv[h].w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int32_t ei = c[h] + q;
+      valid[4 * h + q] = act[h] && ei >= s && ei < e && edge_in_pass(C, ww[q], sg.z < 0);
+      vv[4 * h + q] = cc[q];
+      nd[4 * h + q] = tent(du, ww[q]);
+    }
+  }
+  relax_and_push<8>(I, C, valid, vv, nd, acc, S, lane);
+}
+
 // Vertex work item: up to 32 frontier entries (or far-pile entries on a bucket
 // advance), one per lane; lanes without one pass vin = -1.  Warp-collective.
 template <int BS>
@@ -727,8 +963,12 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
     if (has && lane == __ffs(grp) - 1) atomicAdd(&sm.hist[bin], (uint32_t)__popc(grp));
   }
   if (advance) {
-    const uint32_t mn = __reduce_min_sync(kFull, repush ? du : 0xffffffffu);
-    if (lane == 0 && mn != 0xffffffffu) atomicMin(C.fp_min, mn);
+    if (C.fp_min) {
+      const uint32_t mn = __reduce_min_sync(kFull, repush ? du : 0xffffffffu);
+      if (lane == 0 && mn != 0xffffffffu) atomicMin(C.fp_min, mn);
+    } else if (repush) {
+      S.fmin = min(S.fmin, du);
+    }
     const bool f[1] = {repush};
     const int32_t vv[1] = {rv};
     stage_k<1>(S.fbuf, S.fcnt, f, vv, C.fp, C.fp_tail, I.qcap, &I.ctr->status, lane);
@@ -757,7 +997,9 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
     if (slot < (uint32_t)kBlockListCap) sm.blk[slot] = make_int4(s, e, vtag, (int32_t)(uint32_t)old);
     else wtier = true;  // CTA list full: the warp walks the row itself
   }
-  {
+  if (C.ring) {
+    if (!push_segments(I, gtier, s, e, vtag, lane, S.credit)) wtier = wtier || gtier;  // ring half full: walk it here
+  } else {
     uint32_t slot = 0xffffffffu, b0 = 0, b1 = 0;  // list slot and work items [b0, b1) starting in it
     // one atomicAdd per warp reserves list slots and chunk offsets for all of its
     // grid-tier rows (a per-row atomic on this one counter serialises large frontiers);
@@ -1040,22 +1282,18 @@ __device__ __forceinline__ void level_thresholds(int level, int32_t thr, int32_t
   }
 }
 
-// ---------------------------------------------------------------------------
-// Solve one instance with the CTAs of one team.  I refers to kernel-parameter
-// space (single-instance launches) or to a shared-memory copy (batches).
+// Start of a solve, shared by both schedules: distances and stamps, the initial
+// frontier in q[0] (the source, or the state form's flagged vertices), a team
+// barrier, then the first bucket's width and level (from the policy's start state
+// when the learned policy runs).  Returns false when the run must stop.
 template <int BS>
-__device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS>& sm, uint32_t* bar,
-                               uint32_t& bar_epoch, uint32_t rank, uint32_t team_size, bool& inject) {
-  constexpr int NW = BS / 32;
+__device__ bool start_instance(const LaunchParams& P, const InstDesc& I, Smem<BS>& sm, uint32_t* bar,
+                               uint32_t& bar_epoch, uint32_t rank, uint32_t team_size, bool& inject, bool learned,
+                               uint32_t& base_out, uint32_t& qlen, uint32_t& delta, int& level) {
   Counters* ctr = I.ctr;
   const uint32_t gthreads = team_size * BS;
   const uint32_t gtid = rank * BS + threadIdx.x;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t gwarp = rank * NW + warp;
-  const bool learned = I.policy == NPS_POLICY_LEARNED && P.policy != nullptr;
-  const bool want_iter = learned || (I.trace != nullptr);
-
-  // ---- prologue: distances, stamps, initial frontier
   uint32_t base = __ldcg(I.stamp_base);
   const bool wrap = base > 0xF0000000u;
   if (wrap) base = 0;
@@ -1086,14 +1324,13 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
   if (threadIdx.x == 0) sm.blk_ctr = 0ull;
   const bool inj = inject;
   inject = false;
-  if (!team_barrier<BS>(P, sm, bar, bar_epoch, team_size, &ctr->status, inj)) return;
+  if (!team_barrier<BS>(P, sm, bar, bar_epoch, team_size, &ctr->status, inj)) return false;
 
   if (threadIdx.x == 0) sm.bc_q = __ldcg(&ctr->qtail[0]);
   __syncthreads();
-  uint32_t qlen = min(sm.bc_q, I.qcap);
-  uint32_t it = 0, ep = 0;
-  uint32_t delta = I.dsched ? 1u << (I.dsched & 15u) : I.delta;
-  int level = I.level;
+  qlen = min(sm.bc_q, I.qcap);
+  delta = I.dsched ? 1u << (I.dsched & 15u) : I.delta;
+  level = I.level;
   if (learned) {
     // the first bucket's width and the first level come from the policy too, on the
     // start state.  The first bucket is filled by the source's out-neighbours, so a
@@ -1124,6 +1361,31 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     delta = 1u << sm.pol_choice[0];
     level = sm.pol_choice[1];
   }
+  base_out = base;
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Solve one instance with the CTAs of one team.  I refers to kernel-parameter
+// space (single-instance launches) or to a shared-memory copy (batches).
+template <int BS>
+__device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS>& sm, uint32_t* bar,
+                               uint32_t& bar_epoch, uint32_t rank, uint32_t team_size, bool& inject) {
+  constexpr int NW = BS / 32;
+  Counters* ctr = I.ctr;
+  const uint32_t gthreads = team_size * BS;
+  const uint32_t gtid = rank * BS + threadIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t gwarp = rank * NW + warp;
+  const bool learned = I.policy == NPS_POLICY_LEARNED && P.policy != nullptr;
+  const bool want_iter = learned || (I.trace != nullptr);
+
+  // ---- prologue: distances, stamps, initial frontier, first bucket
+  uint32_t base = 0, qlen = 0, delta = 0;
+  int level = 0;
+  if (!start_instance<BS>(P, I, sm, bar, bar_epoch, rank, team_size, inject, learned, base, qlen, delta, level))
+    return;
+  uint32_t it = 0, ep = 0;
   uint32_t T = delta == 0 ? 0xffffffffu : delta;
   bool advance = false;
   bool heavy_it = false;  // this iteration relaxes the heavy edges of the settle list
@@ -1163,6 +1425,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     C.sstamp = base + hg + 1;
     C.local_rounds = heavy_it ? 0 : I.local_rounds;  // a heavy pass only relaxes heavy edges
     C.order_deg = I.order_degree;
+    C.ring = false;  // queues and lists of the iteration schedule
     level_thresholds(level, I.t1, I.t2, I.t3, C.t_warp, C.t_block, C.t_grid);
     const int4* Hprev = I.heavy + ((it & 1) ? 0 : hhalf);
     const int32_t* Hitem = I.hitem + ((it & 1) ? 0 : I.icap);
@@ -1205,6 +1468,8 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     S.ncnt = 0;
     S.fcnt = 0;
     S.scnt = 0;
+    S.fmin = 0xffffffffu;
+    S.credit = nullptr;  // ring mode only
 
     // ---- work loop: heavy chunk items, then vertex items.  With no more items than
     // warps, warp w takes item w (no atomics); otherwise items come from striped
@@ -1290,7 +1555,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
       if (threadIdx.x == 0) sm.blk_ctr = 0ull;
     }
     NPS_LAP(pc, 5);
-    stage_drain(S, C, I.qcap, &ctr->status, lane);
+    stage_drain(I, S, C, I.qcap, &ctr->status, lane);
     NPS_LAP(pc, 6);
 
     // ---- iteration counters (policy features, trace): warp sums into shared
@@ -1462,6 +1727,384 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
   }
 }
 
+// ---------------------------------------------------------------------------
+// Asynchronous buckets (InstDesc::async).  Inside a bucket nothing waits for a
+// barrier: a vertex improved below the bucket bound goes to the near ring, a row
+// of at least `threshold` edges becomes 256-edge segments on the segment ring,
+// and every warp takes work as soon as it appears -- a segment first, then one of
+// the bucket's static items (32 entries of the far pile being filtered on an
+// advance, or of the initial frontier), then up to 32 near-ring vertices.
+//
+// The bucket ends when its static items are done and the pending total is zero.
+// Ring units (vertices and segments) join the pending total before they become
+// visible, and a warp subtracts the units it took only after everything they
+// pushed has been counted, so the total is zero only when no unit is queued or
+// being processed.  Only then does the team meet at a barrier, to pick the next
+// bucket (the far pile's smallest distance, the policy's width).  Results are
+// exact for the reason the iteration schedule's are: the scheme is
+// label-correcting, and a vertex whose distance drops after it was taken from the
+// ring is queued again -- its mark is reset before its distance is read, the read
+// waiting for the reset by a data dependency, and the mark is set only after the
+// atomicMin that improved the distance has returned.
+//
+// Ring slots carry tags (Vyukov's bounded queue): index i may be written once its
+// slot holds tag i and read once it holds i + 1; a reader then writes i + capacity.
+// Head and tail persist across runs.  A warp claims 32 near-ring indices (or one
+// segment) only while the ring holds unclaimed entries; claims beyond the tail are
+// filled by later pushes, and those still empty when the bucket ends are released
+// by their warp, after which the tail is moved up to the head.
+template <int BS>
+__device__ void solve_instance_async(const LaunchParams& P, const InstDesc& I, Smem<BS>& sm, uint32_t* bar,
+                                     uint32_t& bar_epoch, uint32_t rank, uint32_t team_size, bool& inject) {
+  Counters* ctr = I.ctr;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool learned = I.policy == NPS_POLICY_LEARNED && P.policy != nullptr;
+  const bool want_iter = learned || (I.trace != nullptr);
+  const uint32_t QC = I.nq_mask + 1, SC = I.seg_mask + 1;
+
+  uint32_t base = 0, srclen = 0, delta = 0;
+  int level = 0;
+  if (!start_instance<BS>(P, I, sm, bar, bar_epoch, rank, team_size, inject, learned, base, srclen, delta, level))
+    return;
+  const int32_t* srcq = I.q[0];
+  bool advance = false;
+  uint32_t p = 0;  // bucket (phase) index; its far pushes go to epoch p
+  uint32_t T = delta == 0 ? 0xffffffffu : delta, T_old = 0;
+  Acc tot = {0, 0, 0, 0};
+  PhaseClock pc;
+  pc.reset();
+  uint32_t reached_total = 1;
+
+  for (;;) {
+    IterCtx C;
+    C.T = T;
+    C.snear = base + p + 1;
+    C.sfar = base + p + 1;
+    C.qn = nullptr;
+    C.qn_tail = nullptr;
+    C.fp = I.fq[p & 1];
+    C.fp_tail = &ctr->ftail[p % 3];
+    C.fp_min = nullptr;  // kept per lane in Stage::fmin
+    C.heavy = nullptr;
+    C.heavy_ctr = nullptr;
+    C.hcap = 0;
+    C.hitem = nullptr;
+    C.t_warp = C.t_block = C.t_grid = I.t1;  // GRID tiers: rows of >= threshold edges become segments
+    C.split = 0u;
+    C.heavy_iter = false;
+    C.sq = nullptr;
+    C.sq_tail = &ctr->stail[0];
+    C.sstamp = 0;
+    C.local_rounds = 0;
+    C.order_deg = I.order_degree;
+    C.ring = true;
+    if (rank == 0 && threadIdx.x == 0) {
+      // slots of the next bucket (their last user ended two barriers ago)
+      const uint32_t sl = (p + 1) % 3;
+      ctr->ftail[sl] = 0;
+      ctr->fmin[sl] = 0xffffffffu;
+      ctr->swork[sl] = 0;
+      ctr->sdone[sl] = 0;
+      if (want_iter) {
+        for (int b = 0; b < 8; ++b) ctr->hist[sl][b] = 0;
+        ctr->it_edges[sl] = 0;
+        ctr->it_impr[sl] = 0;
+        ctr->it_reached[sl] = 0;
+      }
+    }
+    if (threadIdx.x < 8) sm.hist[threadIdx.x] = 0;
+    if (threadIdx.x < 3) sm.it_acc[threadIdx.x] = 0;
+    __syncthreads();
+
+    const uint32_t n_static = (srclen + 31) / 32;
+    Acc acc = {0, 0, 0, 0};
+    Stage S;
+    S.nbuf = sm.stage[warp][0];
+    S.fbuf = sm.stage[warp][1];
+    S.sbuf = sm.stage[warp][2];
+    S.ncnt = S.fcnt = S.scnt = 0;
+    S.fmin = 0xffffffffu;
+    S.credit = &sm.credit[warp];
+    if (lane == 0) sm.credit[warp] = 0;
+    uint32_t D = 0;        // ring units taken and processed, not yet subtracted from the pending total
+    uint32_t sdone_w = 0;  // static items processed, not yet added to sdone
+    bool static_left = n_static > 0;
+    uint32_t wb = 0, om = 0;  // claimed near-ring window and its lanes still to read
+    bool has_seg = false;
+    uint32_t sidx = 0;
+    uint32_t idle = 0;
+    unsigned long long t_idle = 0;
+    bool fin = false;
+    for (;;) {
+      bool did = false;
+      // (1) a segment
+      if (!has_seg) {
+        uint32_t got = 0, si = 0;
+        if (lane == 0 && (int32_t)(ld_relaxed_u32(&I.rs->seg_tail) - ld_relaxed_u32(&I.rs->seg_head)) > 0) {
+          si = atomicAdd(&I.rs->seg_head, 1u);
+          got = 1;
+        }
+        if (__shfl_sync(kFull, got, 0)) {
+          has_seg = true;
+          sidx = __shfl_sync(kFull, si, 0);
+        }
+      }
+      if (has_seg) {
+        int4 sg = make_int4(0, 0, 0, 0);
+        uint32_t ready = 0;
+        if (lane == 0) {
+          int4* slot = I.seg + (sidx & I.seg_mask);
+          uint32_t* tag = reinterpret_cast<uint32_t*>(slot) + 3;
+          const uint32_t tg = ld_relaxed_u32(tag);
+          if (tg == sidx + 1) {
+            sg = __ldcg(slot + dep_zero(tg));  // the payload, read after the tag ...
+            // ... and back before the slot is handed back (the store waits for it)
+            st_relaxed_u32(tag + dep_zero((uint32_t)sg.x ^ (uint32_t)sg.y ^ (uint32_t)sg.z), sidx + SC);
+            ready = 1;
+          }
+        }
+        if (__shfl_sync(kFull, ready, 0)) {
+          sg.x = __shfl_sync(kFull, sg.x, 0);
+          sg.y = __shfl_sync(kFull, sg.y, 0);
+          sg.z = __shfl_sync(kFull, sg.z, 0);
+          walk_segment(I, C, sg, acc, S, lane);
+          D += 1;
+          has_seg = false;
+          did = true;
+        }
+      }
+      // (2) a static item
+      if (!did && static_left) {
+        uint32_t t = 0;
+        if (lane == 0) t = atomicAdd(&ctr->swork[p % 3], 1u);
+        t = __shfl_sync(kFull, t, 0);
+        if (t < n_static) {
+          const uint32_t idx = t * 32 + lane;
+          process_vertex_item<BS>(I, C, sm, idx < srclen ? __ldcg(srcq + idx) : -1, advance, T_old, want_iter, acc,
+                                  S, pc, lane);
+          sdone_w += 1;
+          did = true;
+        } else {
+          static_left = false;
+        }
+      }
+      // (3) near-ring vertices
+      if (!did) {
+        if (om == 0) {
+          uint32_t got = 0, b = 0;
+          if (lane == 0 && (int32_t)(ld_relaxed_u32(&I.rs->nq_tail) - ld_relaxed_u32(&I.rs->nq_head)) > 0) {
+            b = atomicAdd(&I.rs->nq_head, 32u);
+            got = 1;
+          }
+          if (__shfl_sync(kFull, got, 0)) {
+            wb = __shfl_sync(kFull, b, 0);
+            om = kFull;
+          }
+        }
+        if (om) {
+          int32_t v = -1;
+          if (om & (1u << lane)) {
+            const uint32_t idx = wb + lane;
+            unsigned long long* slot = I.nq + (idx & I.nq_mask);
+            const unsigned long long x = ld_relaxed_u64p(slot);
+            if ((uint32_t)(x >> 32) == idx + 1) {
+              v = (int32_t)(uint32_t)x;
+              st_relaxed_u64(slot, ((unsigned long long)(idx + QC) << 32) | 0xffffffffull);
+              if ((uint32_t)v >= (uint32_t)I.n) {  // never pushed by a producer: record and drop
+                atomicCAS(&ctr->status, 0u, (uint32_t)NPS_ERR_CAPACITY);
+                v = -1;
+              }
+            }
+          }
+          const uint32_t tm = __ballot_sync(kFull, v >= 0);
+          om &= ~tm;
+          if (tm) {
+            if (v >= 0) {
+              // the mark is reset before the distance is read: a drop after this
+              // exchange queues v again, one before it is seen by the read
+              const uint32_t old = atomicExch(I.mark + v, 0u);
+              v += (int32_t)dep_zero(old);
+            }
+            process_vertex_item<BS>(I, C, sm, v, false, T_old, want_iter, acc, S, pc, lane);
+            D += __popc(tm);
+            did = true;
+          }
+        }
+      }
+      if (did) {
+        idle = 0;
+        continue;
+      }
+      // (4) no work at hand: publish what this warp holds, then test for the end of the bucket
+      stage_drain(I, S, C, I.qcap, &ctr->status, lane);
+      uint32_t f = 0, stop = 0;
+      if (lane == 0) {
+        const uint32_t back = D + sm.credit[warp];  // processed units and unused credits
+        if (sdone_w || back) {
+          __threadfence();  // this warp's pushes are covered before its items and units are done
+          if (sdone_w) atomicAdd(&ctr->sdone[p % 3], sdone_w);
+          if (back) atomicSub(&ctr->pend, back);
+          sm.credit[warp] = 0;
+        }
+        const uint32_t sd = ld_relaxed_u32(&ctr->sdone[p % 3]);
+        if (sd >= n_static) f = ld_relaxed_u32(&ctr->pend + dep_zero(sd)) == 0;
+        if (!f) {
+          const unsigned long long now = globaltimer_ns();
+          if (idle == 0) t_idle = now;
+          if (ld_relaxed_u32(&ctr->status) != 0 || ld_relaxed_u32(P.abort_flag) != 0) {
+            stop = 1;
+          } else if (now - t_idle > P.timeout_ns || now - sm.t_start > P.run_budget_ns) {
+            atomicCAS(&ctr->status, 0u, (uint32_t)NPS_ERR_TIMEOUT);
+            atomicExch(P.abort_flag, 1u);
+            stop = 1;
+          }
+        }
+      }
+      sdone_w = 0;
+      D = 0;
+      if (__shfl_sync(kFull, f, 0)) {
+        fin = true;
+        break;
+      }
+      if (__shfl_sync(kFull, stop, 0)) break;
+      ++idle;
+      __nanosleep(idle < 4 ? 64u : (idle < 12 ? 256u : 1024u));  // idle warps back off the shared counters
+    }
+    if (fin) {
+      // claims never filled: nothing more arrives in this bucket, hand the slots back
+      if (has_seg && lane == 0) st_release_u32(reinterpret_cast<uint32_t*>(I.seg + (sidx & I.seg_mask)) + 3, sidx + SC);
+      if (om & (1u << lane))
+        st_relaxed_u64(I.nq + ((wb + lane) & I.nq_mask), ((unsigned long long)(wb + lane + QC) << 32) | 0xffffffffull);
+    }
+    {
+      const uint32_t fm = __reduce_min_sync(kFull, S.fmin);
+      if (lane == 0 && fm != 0xffffffffu) atomicMin(&ctr->fmin[p % 3], fm);
+    }
+    if (want_iter) {
+      const uint32_t e = __reduce_add_sync(kFull, acc.edges);
+      const uint32_t im = __reduce_add_sync(kFull, acc.impr);
+      const uint32_t rc = __reduce_add_sync(kFull, acc.reached);
+      if (lane == 0) {
+        if (e) atomicAdd(&sm.it_acc[0], e);
+        if (im) atomicAdd(&sm.it_acc[1], im);
+        if (rc) atomicAdd(&sm.it_acc[2], rc);
+      }
+    }
+    tot.edges += acc.edges;
+    tot.impr += acc.impr;
+    tot.reached += acc.reached;
+    tot.processed += acc.processed;
+    __syncthreads();
+    if (fin && rank == 0 && threadIdx.x == 0) {
+      // move the tails up to the heads, past every claim of the bucket: no claim or
+      // push happens any more (a claim needs tail > head, and head >= tail once the
+      // pending total is zero)
+      const uint32_t nh = ld_relaxed_u32(&I.rs->nq_head), nt = ld_relaxed_u32(&I.rs->nq_tail);
+      if ((int32_t)(nh - nt) > 0) atomicExch(&I.rs->nq_tail, nh);
+      const uint32_t sh = ld_relaxed_u32(&I.rs->seg_head), st = ld_relaxed_u32(&I.rs->seg_tail);
+      if ((int32_t)(sh - st) > 0) atomicExch(&I.rs->seg_tail, sh);
+    }
+    if (!team_barrier<BS>(P, sm, bar, bar_epoch, team_size, &ctr->status, false, false,
+                          want_iter ? ctr : nullptr, p % 3))
+      return;
+
+    // ---- the next bucket (every CTA reads the same values)
+    if (threadIdx.x == 0) {
+      const uint32_t sl = p % 3;
+      const uint32_t f1 = __ldcg(&ctr->ftail[sl]);
+      const uint32_t m1 = __ldcg(&ctr->fmin[sl]);
+      const uint32_t st1 = ld_relaxed_u32(&ctr->status);
+      sm.bc_f = f1;
+      sm.bc_m = m1;
+      if (st1 != 0) {
+        atomicExch(P.abort_flag, 1u);
+        sm.ok = 0;
+      }
+      if (want_iter) {
+        uint32_t hb[8];
+        for (int b = 0; b < 8; ++b) hb[b] = __ldcg(&ctr->hist[sl][b]);
+        const unsigned long long ie = __ldcg(&ctr->it_edges[sl]);
+        const unsigned long long ii = __ldcg(&ctr->it_impr[sl]);
+        const uint32_t ir = __ldcg(&ctr->it_reached[sl]);
+        // the iteration schedule's 12 features, over the whole bucket: the next
+        // frontier (the far pile), the degree histogram of the bucket's vertices,
+        // log2(1 + advances), the reached fraction, improvements per scanned edge
+        reached_total += ir;
+        const uint32_t fl0 = min(f1, I.qcap);
+        float hs = 0.f;
+        for (int b = 0; b < 8; ++b) hs += (float)hb[b];
+        const float inv = hs > 0.f ? 1.f / hs : 0.f;
+        float fv[NPS_MLP_IN];
+        fv[0] = log2f(1.f + (float)fl0);
+        for (int b = 0; b < 8; ++b) fv[1 + b] = (float)hb[b] * inv;
+        fv[9] = log2f(1.f + (float)p);
+        fv[10] = (float)reached_total / (float)I.n;
+        fv[11] = ie ? (float)ii / (float)ie : 0.f;
+        if (learned)
+          for (int i = 0; i < NPS_MLP_IN; ++i) sm.feat[i] = (fv[i] - P.policy->mean[i]) * P.policy->istd[i];
+        if (I.trace && rank == 0 && p < I.trace_cap) {
+          nps_trace_rec* tr = I.trace + p;
+          tr->iteration = p;
+          tr->frontier = srclen;
+          tr->far_len = fl0;
+          tr->bucket_hi = T;
+          tr->delta = delta;
+          tr->level = (uint32_t)NPS_LEVEL_GRID | (advance ? 0x200u : 0u) | 0x400u;  // 0x400: asynchronous bucket
+          for (int b = 0; b < 8; ++b) tr->hist[b] = hb[b];
+          tr->edges = ie;
+          tr->improvements = ii;
+          tr->reached = reached_total;
+          tr->heavy = 0;
+          tr->t_ns = globaltimer_ns() - sm.t_start;
+          for (int i = 0; i < NPS_MLP_IN; ++i) tr->feat[i] = fv[i];
+        }
+      }
+    }
+    if (learned && warp == 0) {
+      __syncwarp();
+      if (sm.ok) policy_eval_warp(P.policy, sm.feat, sm.pol_choice, lane);
+    }
+    __syncthreads();
+    if (!sm.ok) return;
+    const uint32_t fl = min(sm.bc_f, I.qcap);
+    p += 1;
+    if (fl == 0) break;
+    // bucket advance: the next bucket filters the far pile of this one
+    if (learned) {
+      delta = 1u << sm.pol_choice[0];
+    } else if (I.dsched) {
+      const uint32_t b = min(p, 7u);  // index of the bucket this advance opens
+      delta = 1u << ((I.dsched >> (4u * b)) & 15u);
+    }
+    const uint32_t fm = sm.bc_m;
+    const uint32_t dstep = delta ? delta : 1u;
+    unsigned long long nt = (unsigned long long)T + dstep;
+    if (fm != 0xffffffffu && (unsigned long long)fm + dstep > nt) nt = (unsigned long long)fm + dstep;
+    T_old = T;
+    T = nt >= 0xffffffffull ? 0xfffffffeu : (uint32_t)nt;
+    advance = true;
+    srcq = I.fq[(p - 1) & 1];
+    srclen = fl;
+  }
+  (void)level;
+
+  // ---- epilogue: totals and the stamp base for the next run on this workspace
+  uint32_t r[4];
+  block_sum4<BS>(sm, tot.edges, tot.impr, tot.reached, tot.processed, r);
+  if (threadIdx.x == 0) {
+    atomicAdd(&ctr->edges, (unsigned long long)r[0]);
+    atomicAdd(&ctr->improvements, (unsigned long long)r[1]);
+    atomicAdd(&ctr->reached, r[2]);
+    atomicAdd(&ctr->processed, (unsigned long long)r[3]);
+    if (rank == 0) {
+      ctr->iterations = p;
+      ctr->solve_ns = globaltimer_ns() - sm.t_start;
+      ctr->buckets = p - 1;
+      *I.stamp_base = base + p + 4;
+    }
+  }
+}
+
 // Resident CTAs per SM the register budget is sized for (about 768-1024
 // threads per SM: enough warps in flight to cover L2 and HBM latency).
 template <int BS>
@@ -1469,8 +2112,10 @@ constexpr int kMinBlocks = BS >= 512 ? 2 : (BS >= 256 ? 3 : 6);
 
 // The persistent kernel.  SINGLE: one instance whose descriptor is the kernel
 // parameter `single` (constant-bank reads in the hot loops); otherwise the
-// team's instances are staged one at a time in shared memory.
-template <int BS, bool SINGLE>
+// team's instances are staged one at a time in shared memory.  ASYNC (single
+// instances only): the asynchronous bucket schedule, in a kernel of its own so
+// that each schedule gets its own register allocation.
+template <int BS, bool SINGLE, bool ASYNC = false>
 __global__ void __launch_bounds__(BS, kMinBlocks<BS>) sssp_persistent_kernel(const __grid_constant__ LaunchParams P,
                                                              const __grid_constant__ InstDesc single) {
   __shared__ Smem<BS> sm;
@@ -1496,7 +2141,9 @@ __global__ void __launch_bounds__(BS, kMinBlocks<BS>) sssp_persistent_kernel(con
   if (threadIdx.x == 0) sm.rank = rank;
   __syncthreads();
   bool inject = P.fault_inject_wait != 0;
-  if constexpr (SINGLE) {
+  if constexpr (SINGLE && ASYNC) {
+    solve_instance_async<BS>(P, single, sm, bar, bar_epoch, rank, (uint32_t)td.cta_count, inject);
+  } else if constexpr (SINGLE) {
     solve_instance<BS>(P, single, sm, bar, bar_epoch, rank, (uint32_t)td.cta_count, inject);
   } else {
     for (int k = 0; k < td.inst_count; ++k) {

@@ -7,6 +7,7 @@
 // allocates five arrays and two queues, and loops on the host until the queue
 // is empty, a call here reuses a cached per-context workspace and makes exactly
 // one persistent launch.  Errors come back as status codes instead of exit().
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -44,6 +45,36 @@ nps_status nps_fail(nps_status code, const std::string& msg) {
 void nps_clear_error() { g_last_error.clear(); }
 
 extern "C" const char* nps_last_error_string(void) { return g_last_error.c_str(); }
+
+// Driver entry points through the runtime (the library links no libcuda).
+unsigned long long nps_context_id(int device) {
+  using GetCurrentFn = CUresult (*)(CUcontext*);
+  using GetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrentFn get_current = nullptr;
+  static GetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetIdFn>(f);
+    cudaGetLastError();
+  });
+  if (!get_current || !get_id) return 0;
+  if (cudaSetDevice(device) != cudaSuccess || cudaFree(nullptr) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  CUcontext cu = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&cu) != CUDA_SUCCESS || !cu || get_id(cu, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 extern "C" int32_t nps_abi_version(void) { return NPS_ABI_VERSION; }
 
 #define NPS_CUDA(call)                                                                       \
@@ -120,11 +151,17 @@ nps_status device_info(int dev, DevInfo* out) {
 
 using KernelFn = void (*)(const LaunchParams, const InstDesc);
 
-KernelFn pick_kernel(int bs, bool single) {
+KernelFn pick_kernel(int bs, bool single, bool async = false) {
   switch (bs) {
-    case 128: return single ? nps::sssp_persistent_kernel<128, true> : nps::sssp_persistent_kernel<128, false>;
-    case 256: return single ? nps::sssp_persistent_kernel<256, true> : nps::sssp_persistent_kernel<256, false>;
-    case 512: return single ? nps::sssp_persistent_kernel<512, true> : nps::sssp_persistent_kernel<512, false>;
+    case 128:
+      return async ? nps::sssp_persistent_kernel<128, true, true>
+                   : (single ? nps::sssp_persistent_kernel<128, true> : nps::sssp_persistent_kernel<128, false>);
+    case 256:
+      return async ? nps::sssp_persistent_kernel<256, true, true>
+                   : (single ? nps::sssp_persistent_kernel<256, true> : nps::sssp_persistent_kernel<256, false>);
+    case 512:
+      return async ? nps::sssp_persistent_kernel<512, true, true>
+                   : (single ? nps::sssp_persistent_kernel<512, true> : nps::sssp_persistent_kernel<512, false>);
     default: return nullptr;
   }
 }
@@ -157,8 +194,9 @@ cudaError_t set_carveout(int dev, KernelFn k, int bs, int nb) {
   return cudaSuccess;
 }
 
-nps_status grid_size(int dev, const DevInfo& di, int bs, bool single, int ctas_per_sm, int* grid) {
-  KernelFn k = pick_kernel(bs, single);
+nps_status grid_size(int dev, const DevInfo& di, int bs, bool single, int ctas_per_sm, int* grid,
+                     bool async = false) {
+  KernelFn k = pick_kernel(bs, single, async);
   if (!k) return nps_fail(NPS_ERR_INVALID_ARG, "block_size must be 128, 256 or 512");
   int nb = 0;
   NPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)k, bs, 0));
@@ -222,6 +260,8 @@ struct Control {
 
 struct PolicyState {
   PolicyDev* dev = nullptr;
+  PolicyDev host;                 // kept to upload again after a device reset
+  unsigned long long ctx_id = 0;  // context `dev` was allocated in
   bool set = false;
 };
 
@@ -232,12 +272,18 @@ std::vector<PolicyState> g_policy;
 
 struct nps_ctx {
   int device = 0;
+  unsigned long long ctx_id = 0;  // context the cached state below lives in (nps_context_id)
   cudaStream_t stream = nullptr;
   DevInfo di;
   // per-instance workspace (single-instance calls)
   DevBuf<int32_t> q0, q1, f0, f1, s0, s1;
   DevBuf<uint32_t> mark, fmark, smark, stamp;
   DevBuf<int4> heavy;
+  // work rings of the asynchronous schedule (tags and head/tail persist across runs)
+  DevBuf<unsigned long long> nq;
+  DevBuf<int4> segs;
+  DevBuf<nps::RingState> rstate;
+  bool rings_ready = false;
   DevBuf<char> control;
   DevBuf<nps_trace_rec> trace;
   uint32_t trace_count = 0;
@@ -291,6 +337,9 @@ void ctx_release(nps_ctx* c) {
     b->release();
   for (auto* b : {&c->mark, &c->fmark, &c->smark, &c->stamp, &c->g_w, &c->g_dist, &c->b_stamp}) b->release();
   c->heavy.release();
+  c->nq.release();
+  c->segs.release();
+  c->rstate.release();
   c->b_heavy.release();
   c->control.release();
   c->b_control.release();
@@ -325,6 +374,12 @@ nps_status default_ctx(int device, nps_ctx** out) {
   std::lock_guard<std::mutex> lk(g_ctx_mu);
   if (device < 0) return nps_fail(NPS_ERR_INVALID_ARG, "device ordinal out of range");
   if ((int)g_default_ctx.size() <= device) g_default_ctx.resize(device + 1, nullptr);
+  const unsigned long long id = nps_context_id(device);
+  if (g_default_ctx[device] && id != 0 && g_default_ctx[device]->ctx_id != id) {
+    // the device was reset: its buffers, stream and events died with the old
+    // context, so the cached state is dropped without being freed
+    g_default_ctx[device] = nullptr;
+  }
   if (!g_default_ctx[device]) {
     auto* c = new nps_ctx();
     nps_status st = ctx_init(c, device);
@@ -332,6 +387,7 @@ nps_status default_ctx(int device, nps_ctx** out) {
       delete c;
       return st;
     }
+    c->ctx_id = id;
     g_default_ctx[device] = c;
   }
   *out = g_default_ctx[device];
@@ -372,7 +428,21 @@ uint32_t heavy_capacity(int32_t n, int64_t m, const nps_params& p) {
 PolicyDev* policy_ptr(int device) {
   std::lock_guard<std::mutex> lk(g_policy_mu);
   if ((int)g_policy.size() <= device || !g_policy[device].set) return nullptr;
-  return g_policy[device].dev;
+  PolicyState& ps = g_policy[device];
+  const unsigned long long id = nps_context_id(device);
+  if (id != 0 && id != ps.ctx_id) {
+    // the device was reset since the weights were uploaded: upload them again
+    ps.dev = nullptr;
+    if (cudaMalloc(&ps.dev, sizeof(PolicyDev)) != cudaSuccess ||
+        cudaMemcpy(ps.dev, &ps.host, sizeof(PolicyDev), cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaGetLastError();
+      ps.dev = nullptr;
+      ps.set = false;
+      return nullptr;
+    }
+    ps.ctx_id = id;
+  }
+  return ps.dev;
 }
 
 void fill_thresholds(const nps_params& p, InstDesc& d) {
@@ -388,6 +458,42 @@ void fill_thresholds(const nps_params& p, InstDesc& d) {
   d.dsched = p.delta_schedule;
 }
 
+// Whether a single-instance call runs the asynchronous schedule: requested, tiers
+// at the grid level (or chosen by the learned policy, which then runs grid tiers),
+// no warp-local rounds and no light/heavy split in effect.
+bool use_async(const nps_params& p) {
+  if (p.schedule != NPS_SCHEDULE_ASYNC) return false;
+  if (p.level != NPS_LEVEL_GRID && p.policy != NPS_POLICY_LEARNED) return false;
+  if (p.local_rounds != 0) return false;
+  const bool split = p.light_heavy && (p.delta != 0 || p.delta_schedule != 0 || p.policy == NPS_POLICY_LEARNED);
+  return !split;
+}
+
+size_t pow2_at_least(size_t x) {
+  size_t r = 1;
+  while (r < x) r <<= 1;
+  return r;
+}
+
+// Ring capacities: the near ring holds every vertex at most once at a time plus the
+// claims of every warp, so 2n + 2^18 slots leave it at most half full; the segment
+// ring is sized so that half of it holds 2 m / 256 + 2^11 segments (pushes back off
+// to the pushing warp beyond half).
+size_t near_ring_slots(int32_t n) { return pow2_at_least((size_t)2 * (size_t)n + ((size_t)1 << 18)); }
+size_t seg_ring_slots(int64_t m) { return pow2_at_least(std::max<size_t>((size_t)1 << 14, (size_t)m / 64 + 4096)); }
+
+// Tags to their first lap (slot i free for index i), heads and tails to zero.
+__global__ void ring_init_kernel(unsigned long long* nq, uint32_t qc, int4* seg, uint32_t sc, nps::RingState* rs) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < qc; i += stride)
+    nq[i] = ((unsigned long long)i << 32) | 0xffffffffull;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < sc; i += stride) seg[i] = make_int4(0, 0, 0, (int)i);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    rs->nq_head = rs->nq_tail = 0;
+    rs->seg_head = rs->seg_tail = 0;
+  }
+}
+
 // Whole-launch bound: 30 per-wait timeouts, at least 60 s.
 unsigned long long run_budget_ns(const nps_params& p) {
   return (unsigned long long)(std::max(60.0, 30.0 * p.timeout_s) * 1e9);
@@ -395,7 +501,7 @@ unsigned long long run_budget_ns(const nps_params& p) {
 
 nps_status launch(nps_ctx* c, cudaStream_t s, int bs, bool single, int grid, const LaunchParams& lp,
                   const InstDesc& inst) {
-  KernelFn k = pick_kernel(bs, single);
+  KernelFn k = pick_kernel(bs, single, single && inst.async != 0);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)grid);
   cfg.blockDim = dim3((unsigned)bs);
@@ -440,7 +546,7 @@ nps_status run_single(nps_ctx* c, cudaStream_t s, const int32_t* row, const int3
   nps_heavy_items(m, hcap / 2, 0, &icap, &ishift);
   if ((e = c->heavy.ensure(nps_heavy_slots(hcap, icap), false, s))) return e;
   int grid = 0;
-  if ((e = grid_size(c->device, c->di, p.block_size, true, p.ctas_per_sm, &grid))) return e;
+  if ((e = grid_size(c->device, c->di, p.block_size, true, p.ctas_per_sm, &grid, use_async(p)))) return e;
   Control ctl(1, 1, grid);
   if ((e = c->control.ensure(ctl.bytes(), false, s))) return e;
   ctl.base = c->control.p;
@@ -448,6 +554,25 @@ nps_status run_single(nps_ctx* c, cudaStream_t s, const int32_t* row, const int3
     if ((e = c->trace.ensure(1 << 16, false, s))) return e;
   }
   if ((e = ensure_pinned_counters(c, 1))) return e;
+  const bool async = use_async(p);
+  size_t qc = 0, sc = 0;
+  if (async) {
+    qc = near_ring_slots(n);
+    sc = seg_ring_slots(m);
+    if (qc > ((size_t)1 << 31) || sc > ((size_t)1 << 31))
+      return nps_fail(NPS_ERR_INVALID_ARG, "asynchronous schedule: graph too large for 32-bit ring indices");
+    const void *q0 = c->nq.p, *s0 = c->segs.p;
+    if ((e = c->nq.ensure(qc, false, s)) || (e = c->segs.ensure(sc, false, s)) || (e = c->rstate.ensure(1, false, s)))
+      return e;
+    if (c->nq.p != q0 || c->segs.p != s0) c->rings_ready = false;
+    qc = c->nq.n;
+    sc = c->segs.n;
+    if (!c->rings_ready) {
+      ring_init_kernel<<<c->di.sms * 4, 256, 0, s>>>(c->nq.p, (uint32_t)qc, c->segs.p, (uint32_t)sc, c->rstate.p);
+      NPS_CUDA(cudaGetLastError());
+      c->rings_ready = true;
+    }
+  }
 
   InstDesc d;
   memset(&d, 0, sizeof(d));
@@ -481,6 +606,15 @@ nps_status run_single(nps_ctx* c, cudaStream_t s, const int32_t* row, const int3
   d.trace_cap = p.trace ? (uint32_t)c->trace.n : 0;
   d.vec_ok = (((uintptr_t)col | (uintptr_t)w) & 15) == 0;
   fill_thresholds(p, d);
+  if (async) {
+    d.async = 1;
+    d.nq = c->nq.p;
+    d.nq_mask = (uint32_t)(qc - 1);
+    d.seg = c->segs.p;
+    d.seg_mask = (uint32_t)(sc - 1);
+    d.rs = c->rstate.p;
+    d.wait_ns = (unsigned long long)(p.timeout_s * 1e9);
+  }
 
   TeamDesc td{0, grid, 0, 1};
   // single-instance launches read the team table from a small device buffer
@@ -515,6 +649,7 @@ nps_status run_single(nps_ctx* c, cudaStream_t s, const int32_t* row, const int3
 // A launch that stopped early never advanced its stamp base, so its stamps
 // could collide with the next run's: clear marks and base after any failure.
 void reset_stamps(nps_ctx* c, cudaStream_t s) {
+  c->rings_ready = false;  // a stopped asynchronous run leaves its ring claims unreleased
   if (c->mark.p) cudaMemsetAsync(c->mark.p, 0, c->mark.n * sizeof(uint32_t), s);
   if (c->fmark.p) cudaMemsetAsync(c->fmark.p, 0, c->fmark.n * sizeof(uint32_t), s);
   if (c->smark.p) cudaMemsetAsync(c->smark.p, 0, c->smark.n * sizeof(uint32_t), s);
@@ -1000,12 +1135,17 @@ extern "C" nps_status nps_policy_set_weights(int32_t device, const float* w1, co
   memcpy(h.b2, b2, sizeof(h.b2));
   memcpy(h.mean, mean, sizeof(h.mean));
   memcpy(h.istd, istd, sizeof(h.istd));
+  const unsigned long long id = nps_context_id(device);
   std::lock_guard<std::mutex> lk(g_policy_mu);
   if ((int)g_policy.size() <= device) g_policy.resize(device + 1);
+  PolicyState& ps = g_policy[device];
   NPS_CUDA(cudaSetDevice(device));
-  if (!g_policy[device].dev) NPS_CUDA(cudaMalloc(&g_policy[device].dev, sizeof(PolicyDev)));
-  NPS_CUDA(cudaMemcpy(g_policy[device].dev, &h, sizeof(h), cudaMemcpyHostToDevice));
-  g_policy[device].set = true;
+  if (ps.dev && ps.ctx_id != id) ps.dev = nullptr;  // allocated before a device reset: gone
+  if (!ps.dev) NPS_CUDA(cudaMalloc(&ps.dev, sizeof(PolicyDev)));
+  NPS_CUDA(cudaMemcpy(ps.dev, &h, sizeof(h), cudaMemcpyHostToDevice));
+  ps.host = h;
+  ps.ctx_id = id;
+  ps.set = true;
   return NPS_OK;
 }
 

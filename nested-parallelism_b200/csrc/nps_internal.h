@@ -65,6 +65,14 @@ nps_status nps_ensure(T** p, size_t* have, size_t want, cudaStream_t s, const ch
   return NPS_OK;
 }
 
+// Identifier of the context current on `device` (made current, and created if a
+// reset destroyed it), 0 if it cannot be read.  Every per-device cache of the
+// library remembers the identifier it was built under: a different one means the
+// device was reset since -- the reference's prepare_gpu() calls cudaDeviceReset()
+// before every run -- and the cached device memory, streams and events are gone,
+// so the cache is abandoned (not freed) and built again.
+unsigned long long nps_context_id(int device);
+
 // Device copy of the learned-policy weights of `device` (null if none loaded).
 const void* nps_policy_device_weights(int device);
 

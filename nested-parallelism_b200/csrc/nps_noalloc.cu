@@ -21,9 +21,9 @@
 // Every GPU that loads libnps holds this array until the process exits.  The
 // array's host-side name is only a stand-in for the symbol, not a device
 // address, so the first call on each device resolves the address with
-// cudaGetSymbolAddress (that device current) and caches it for the life of the
-// process.  cudaDeviceReset() unloads the module and invalidates that address:
-// do not use this entry point after resetting a device it has run on.
+// cudaGetSymbolAddress (that device current) and caches it; after a
+// cudaDeviceReset() of that device the module is loaded anew, so the address is
+// resolved again on the next call.
 //
 // Sharing.  All calls on a device share the one array and it keeps the state of
 // the last call: counters and barrier words are cleared at the start of each
@@ -80,11 +80,16 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 unsigned char* g_addr[kMaxDevices] = {nullptr};
+unsigned long long g_addr_ctx[kMaxDevices] = {0};  // context each address was resolved in
 
-// Device address of the scratch on `device` (which must be current).
+// Device address of the scratch on `device` (which must be current), resolved
+// again when the device was reset since (the module is loaded anew then).
 nps_status scratch_address(int device, unsigned char** out) {
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_addr[device]) {
+  const unsigned long long id = nps_context_id(device);
+  if (!g_addr[device] || (id != 0 && id != g_addr_ctx[device])) {
+    g_addr[device] = nullptr;
+    g_addr_ctx[device] = id;
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_nps_noalloc_scratch);
     if (e != cudaSuccess || !p)

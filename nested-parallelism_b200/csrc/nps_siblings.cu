@@ -333,6 +333,7 @@ __global__ void __launch_bounds__(kGenThreads) reached_kernel(Graph g, SibCtr* c
 
 // Per-device cached workspace.
 struct SibWork {
+  unsigned long long ctx_id = 0;  // context the cached buffers live in (nps_context_id)
   std::mutex mu;
   cudaStream_t stream = nullptr;
   int32_t* q = nullptr;
@@ -363,7 +364,14 @@ std::vector<SibWork*> g_sib;
 SibWork* sib_work(int device) {
   std::lock_guard<std::mutex> lk(g_sib_mu);
   if ((int)g_sib.size() <= device) g_sib.resize(device + 1, nullptr);
-  if (!g_sib[device]) g_sib[device] = new SibWork();
+  {
+    const unsigned long long id = nps_context_id(device);
+    if (g_sib[device] && id != 0 && g_sib[device]->ctx_id != id) g_sib[device] = nullptr;  // device reset: abandoned
+    if (!g_sib[device]) {
+      g_sib[device] = new SibWork();
+      g_sib[device]->ctx_id = id;
+    }
+  }
   return g_sib[device];
 }
 

@@ -420,6 +420,7 @@ __global__ void __launch_bounds__(kThreads, kChunkCtas) spmv_chunks_kernel(Mat A
 
 
 struct SpmvWork {
+  unsigned long long ctx_id = 0;  // context the cached buffers live in (nps_context_id)
   std::mutex mu;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[4] = {};
@@ -460,7 +461,14 @@ nps_status spmv_work(int device, SpmvWork** out) {
   {
     std::lock_guard<std::mutex> lk(g_spmv_mu);
     if ((int)g_spmv.size() <= device) g_spmv.resize(device + 1, nullptr);
-    if (!g_spmv[device]) g_spmv[device] = new SpmvWork();
+    {
+    const unsigned long long id = nps_context_id(device);
+    if (g_spmv[device] && id != 0 && g_spmv[device]->ctx_id != id) g_spmv[device] = nullptr;  // device reset: abandoned
+    if (!g_spmv[device]) {
+      g_spmv[device] = new SpmvWork();
+      g_spmv[device]->ctx_id = id;
+    }
+  }
     w = g_spmv[device];
   }
   *out = w;
