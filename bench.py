@@ -1156,7 +1156,10 @@ def bench_rmat_eval(a, ws, rank, local, wl, desc):
     if use_learned:
         pol.load_into_kernel(pol.MLPWeights.load(wpath), local)
     tune_log = []
-    plain = nps.Params(device=local, **prm)
+    sched = nps.SCHEDULE_ASYNC if a.schedule == "async" else nps.SCHEDULE_ITERATIONS
+    if sched == nps.SCHEDULE_ASYNC:
+        prm["light_heavy"] = False
+    plain = nps.Params(device=local, schedule=sched, **prm)
     learned = dataclasses.replace(plain, policy=nps.POLICY_LEARNED, light_heavy=False, order_degree=0,
                                   delta_schedule=0) if use_learned else None
     if a.tune_budget > 0 and a.delta is None and a.level is None:
@@ -1354,6 +1357,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--tune-budget", type=int, default=24, help="autotuner evaluations before timing")
     ap.add_argument("--seeds", default=None, help="rmat22 only: comma-separated subset of the evaluation seeds")
+    ap.add_argument("--schedule", default="iterations", choices=["iterations", "async"],
+                    help="SSSP schedule of both arms: frontier iterations with a team barrier each, or asynchronous "
+                         "buckets (NPS_SCHEDULE_ASYNC)")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     a.seeds = tuple(int(x) for x in a.seeds.split(",")) if a.seeds else None
@@ -1387,6 +1393,9 @@ def main():
         prm["delta"] = a.delta
     if a.level is not None:
         prm["level"] = a.level
+    if a.schedule == "async":
+        prm["schedule"] = 1  # NPS_SCHEDULE_ASYNC
+        prm["light_heavy"] = False
 
     if a.impl == "reference":
         if rank != 0:

@@ -58,7 +58,7 @@ extern "C" {
 #endif
 
 #define NPS_INF 0x40000000u  /* 1<<30, apps/sssp/src/gpu/sssp_wrapper.cu:7 */
-#define NPS_ABI_VERSION 1
+#define NPS_ABI_VERSION 2
 
 typedef int32_t nps_status;
 enum {
@@ -88,6 +88,14 @@ enum {
   NPS_POLICY_LEARNED = 1   /* bucket widths (first from the start state, then at each advance) and the level of
                               every iteration from the MLP loaded with nps_policy_set_weights; error if none */
 };
+
+/* The learned policy runs only on graphs of at least this many edges (unless
+ * nps_params.policy_min_edges says otherwise); smaller ones run the plain kernel with
+ * the same parameters (stats.policy_used says which).
+ * Measured on held-out R-MAT graphs: below about 6 M edges (scale 18 at edge
+ * factor 16) the policy's per-iteration cost outweighs what its bucket widths
+ * save, above it the widths win (scale 19: 1.09x, 20: 1.23x, 22: 1.45x). */
+#define NPS_POLICY_MIN_EDGES 6000000
 
 typedef struct nps_params {
   int32_t level;            /* NPS_LEVEL_* (default NPS_LEVEL_BLOCK, the reference Makefile's CONSOLIDATE_LEVEL=1) */
@@ -119,6 +127,9 @@ typedef struct nps_params {
                                reserved[1] > 0: nps_bc folds at most this many sources per block
                                of dependency rows (0 = as many as 2 GB of rows hold) */
   int32_t schedule;         /* NPS_SCHEDULE_* (default NPS_SCHEDULE_ITERATIONS) */
+  int64_t policy_min_edges; /* NPS_POLICY_LEARNED runs only on graphs of at least this many edges,
+                               smaller ones run the plain kernel; 0 (default) = NPS_POLICY_MIN_EDGES,
+                               negative = no minimum */
 } nps_params;
 
 /* How the persistent SSSP kernel moves from one frontier to the next. */
@@ -139,7 +150,8 @@ typedef struct nps_stats {
   uint64_t improvements;    /* successful atomicMin relaxations */
   uint64_t vertices_processed;
   uint32_t reached;         /* vertices with a finite distance */
-  uint32_t pad0;
+  uint32_t policy_used;     /* NPS_POLICY_* the run used (NPS_POLICY_PLAIN when the learned policy was
+                               asked for on a graph below NPS_POLICY_MIN_EDGES edges) */
   uint64_t reached_edges;   /* out-edges of reached vertices (m_r) */
   float kernel_ms;          /* device time of the persistent launch (CUDA events); per instance of a
                                batch: device time from the launch to the end of that instance's solve */

@@ -223,6 +223,7 @@ class Params:
     fault_inject_wait: bool = False     # test hook: the first barrier can never complete
     bc_block_sources: int = 0           # bc: sources per block of dependency rows (0 = as memory allows)
     schedule: int = 0                   # SCHEDULE_ITERATIONS or SCHEDULE_ASYNC (see include/nps.h)
+    policy_min_edges: int = 0           # learned policy only from this many edges (0: library default, <0: none)
 
     def to_c(self, device_ptrs: bool, stream: Optional[int] = None) -> nps_params:
         p = nps_params()
@@ -241,6 +242,7 @@ class Params:
         p.reserved[0] = int(bool(self.fault_inject_wait))
         p.reserved[1] = int(self.bc_block_sources)
         p.schedule = int(self.schedule)
+        p.policy_min_edges = int(self.policy_min_edges)
         return p
 
 
@@ -257,12 +259,14 @@ class Stats:
     status: int = 0
     grid_ctas: int = 0
     phase_cycles: tuple = ()
+    policy_used: int = 0
 
     @staticmethod
     def from_c(s: nps_stats) -> "Stats":
         return Stats(int(s.iterations), int(s.buckets), int(s.edges_scanned), int(s.improvements),
                      int(s.vertices_processed), int(s.reached), float(s.kernel_ms), float(s.total_ms),
-                     int(s.status), int(s.grid_ctas), tuple(int(x) for x in s.phase_cycles))
+                     int(s.status), int(s.grid_ctas), tuple(int(x) for x in s.phase_cycles),
+                     int(s.policy_used))
 
 
 def _ptr(x) -> int:

@@ -36,7 +36,7 @@ class nps_params(C.Structure):
         ("device", C.c_int32), ("stream", C.c_void_p), ("timeout_s", C.c_double),
         ("trace", C.c_int32), ("light_heavy", C.c_int32), ("local_rounds", C.c_int32),
         ("order_degree", C.c_int32), ("delta_schedule", C.c_uint32), ("reserved", C.c_int32 * 2),
-        ("schedule", C.c_int32),
+        ("schedule", C.c_int32), ("policy_min_edges", C.c_int64),
     ]
 
 
@@ -44,7 +44,7 @@ class nps_stats(C.Structure):
     _fields_ = [
         ("iterations", C.c_uint32), ("buckets", C.c_uint32), ("edges_scanned", C.c_uint64),
         ("improvements", C.c_uint64), ("vertices_processed", C.c_uint64), ("reached", C.c_uint32),
-        ("pad0", C.c_uint32), ("reached_edges", C.c_uint64), ("kernel_ms", C.c_float),
+        ("policy_used", C.c_uint32), ("reached_edges", C.c_uint64), ("kernel_ms", C.c_float),
         ("total_ms", C.c_float), ("status", C.c_int32), ("grid_ctas", C.c_int32),
         ("phase_cycles", C.c_uint64 * 9),
     ]

@@ -217,12 +217,33 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64p(const unsigned lon
   return v;
 }
 
+__device__ __forceinline__ int4 ld_relaxed_v4(const int4* p) {
+  int4 v;
+  asm volatile("ld.relaxed.gpu.global.v4.s32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(p)
+               : "memory");
+  return v;
+}
+
 __device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
   asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 __device__ __forceinline__ void st_relaxed_u32(uint32_t* p, uint32_t v) {
   asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ uint32_t atom_exch_release(uint32_t* p, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.release.gpu.global.exch.b32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ uint32_t atom_exch_acquire(uint32_t* p, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.acquire.gpu.global.exch.b32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
 }
 
 __device__ __forceinline__ void st_release_u32(uint32_t* p, uint32_t v) {
@@ -438,9 +459,10 @@ __device__ __forceinline__ void relax_batch(const InstDesc& I, const IterCtx& C,
       bool near = nd[j] < C.T;
       if (!near && C.order_deg > 0) near = __ldg(I.row_ptr + v[j] + 1) - __ldg(I.row_ptr + v[j]) < C.order_deg;
       if (near) {
-        // (ring mode: the exchange is issued only once this atomicMin has returned, so a
-        // consumer that sees the mark set sees the new distance too)
-        pn[j] = atomicExch(I.mark + v[j], C.snear) != C.snear;
+        // ring mode: a consumer resets the mark before it reads the distance, so the
+        // mark is set with release semantics -- whoever sees it set sees this atomicMin
+        // (ordering by the dependency on the returned value alone lost updates on B200)
+        pn[j] = (C.ring ? atom_exch_release(I.mark + v[j], C.snear) : atomicExch(I.mark + v[j], C.snear)) != C.snear;
       } else {
         pf[j] = atomicExch(I.fmark + v[j], C.sfar) != C.sfar;
       }
@@ -704,8 +726,11 @@ struct Smem {
   uint32_t red[4][BS / 32];
   float feat[NPS_MLP_IN];
   int32_t pol_choice[2];
+  PolicyDev pol;               // the policy's weights, copied once per solve (learned runs only)
   uint32_t it_acc[3];          // this CTA's edges, improvements, first reaches in the iteration
   uint32_t credit[BS / 32];    // ring mode: pending-total credits held per warp
+  uint32_t phase_flag;         // ring mode: set by the CTA's warp 0 when the bucket ends (p + 1) or
+                               // must stop (0xffffffff); the CTA's other warps read it, not global memory
   TeamDesc team;
   int32_t team_id;
   uint32_t rank;
@@ -817,15 +842,17 @@ __device__ __forceinline__ void warp_row(const InstDesc& I, const IterCtx& C, in
   }
 }
 
-// Ring mode: the grid-tier rows of a warp become segments of at most 256 edges
-// (64 chunks from the row's 4-aligned start) on the segment ring.  The segments
+constexpr int kSegEdges = 1024;  // edges per segment: four 256-edge rounds of one warp
+
+// Ring mode: the grid-tier rows of a warp become segments of at most kSegEdges
+// edges (from the row's 4-aligned start) on the segment ring.  The segments
 // are covered by pending-total credits before they are visible; one reservation
 // per warp.
 // Returns false, pushing nothing, when the ring is more than half full: the rows
 // are then walked by the warp itself.  Warp-collective.
 __device__ __forceinline__ bool push_segments(const InstDesc& I, bool gtier, int32_t s, int32_t e, int32_t vtag,
                                               int lane, uint32_t* credit) {
-  const uint32_t nseg = gtier ? (uint32_t)(((int64_t)e - (s & ~3) + 255) >> 8) : 0u;
+  const uint32_t nseg = gtier ? (uint32_t)(((int64_t)e - (s & ~3) + kSegEdges - 1) / kSegEdges) : 0u;
   uint32_t incl = nseg;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -861,9 +888,10 @@ __device__ __forceinline__ bool push_segments(const InstDesc& I, bool gtier, int
       uint32_t* tag = reinterpret_cast<uint32_t*>(slot) + 3;
       if (ld_relaxed_u32(tag) == idx || ring_wait_tag(tag, idx, I)) {
         int32_t* w = reinterpret_cast<int32_t*>(slot);
-        w[0] = (int32_t)max((int64_t)rs, c0 + 256 * (int64_t)j);
-        w[1] = (int32_t)min((int64_t)re, c0 + 256 * ((int64_t)j + 1));
-        w[2] = rz;
+        st_relaxed_u32(reinterpret_cast<uint32_t*>(w), (uint32_t)max((int64_t)rs, c0 + kSegEdges * (int64_t)j));
+        st_relaxed_u32(reinterpret_cast<uint32_t*>(w) + 1,
+                       (uint32_t)min((int64_t)re, c0 + kSegEdges * ((int64_t)j + 1)));
+        st_relaxed_u32(reinterpret_cast<uint32_t*>(w) + 2, (uint32_t)rz);
       }
     }
   }
@@ -883,23 +911,17 @@ __device__ __forceinline__ bool push_segments(const InstDesc& I, bool gtier, int
   return true;
 }
 
-// One segment {start, end, vertex | heavy flag} of at most 256 edges starting at a
-// 4-aligned chunk: two chunks per lane, one batch of eight candidates.  The owner's
-// distance is read now (it may have dropped since the segment was pushed; the owner
-// is then queued again for the drop).  Warp-collective.
-__device__ __forceinline__ void walk_segment(const InstDesc& I, const IterCtx& C, int4 sg, Acc& acc, Stage& S,
-                                             int lane) {
-  const int32_t s = sg.x, e = sg.y;
-  const uint32_t v = (uint32_t)sg.z & 0x7fffffffu;
-  const uint32_t du = v < (uint32_t)I.n ? __ldcg(I.dist + v) : kInf;
-  const int32_t c0 = s & ~3;
+// 256 edges from chunk r0 of the row range [s, e): two chunks per lane, their
+// column and weight loads issued together, one batch of eight candidates.
+__device__ __forceinline__ void walk_round(const InstDesc& I, const IterCtx& C, int32_t r0, int32_t s, int32_t e,
+                                           uint32_t du, bool heavy, Acc& acc, Stage& S, int lane) {
   bool act[2];
   int32_t c[2];
   int4 cv[2], wv[2];
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
-    c[h] = c0 + 128 * h + 4 * lane;
-    act[h] = s >= 0 && e <= I.m && c[h] < e;
+    c[h] = r0 + 128 * h + 4 * lane;
+    act[h] = c[h] < e;
     load_chunk(I, act[h], c[h], s, e, cv[h], wv[h]);
   }
   bool valid[8];
@@ -912,12 +934,29 @@ __device__ __forceinline__ void walk_segment(const InstDesc& I, const IterCtx& C
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int32_t ei = c[h] + q;
-      valid[4 * h + q] = act[h] && ei >= s && ei < e && edge_in_pass(C, ww[q], sg.z < 0);
+      valid[4 * h + q] = act[h] && ei >= s && ei < e && edge_in_pass(C, ww[q], heavy);
       vv[4 * h + q] = cc[q];
       nd[4 * h + q] = tent(du, ww[q]);
     }
   }
   relax_and_push<8>(I, C, valid, vv, nd, acc, S, lane);
+}
+
+// One segment {start, end, vertex | heavy flag} of at most kSegEdges edges from a
+// 4-aligned chunk, in rounds of 256 edges: two chunks per lane, one batch of eight
+// candidates per round.  The owner's distance is read now, by a load that sees the
+// latest value (a weak load could return a copy older than the one the owner's
+// consumer read, and the edges would miss that improvement).  Warp-collective.
+__device__ __forceinline__ void walk_segment(const InstDesc& I, const IterCtx& C, int4 sg, Acc& acc, Stage& S,
+                                             int lane) {
+  const int32_t s = sg.x, e = sg.y;
+  const uint32_t v = (uint32_t)sg.z & 0x7fffffffu;
+  if (s < 0 || e > I.m || v >= (uint32_t)I.n) {  // never pushed by a producer: record and skip
+    if (lane == 0) atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_CAPACITY);
+    return;
+  }
+  const uint32_t du = ld_relaxed_u32(I.dist + v);
+  for (int32_t r0 = s & ~3; r0 < e; r0 += 256) walk_round(I, C, r0, s, e, du, sg.z < 0, acc, S, lane);
 }
 
 // Vertex work item: up to 32 frontier entries (or far-pile entries on a bucket
@@ -932,7 +971,9 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
   bool repush = false;
   int32_t rv = 0;
   if (v >= 0) {
-    du = __ldcg(I.dist + v);
+    // ring mode: a load that sees the latest distance (the mark-reset protocol needs
+    // the value as of the reset; a weak load may return an older copy)
+    du = C.ring ? ld_relaxed_u32(I.dist + v) : __ldcg(I.dist + v);
     if (advance) {
       // far-pile entry: stale below the old bound, deferred again at/above the new one
       if (du < T_old) {
@@ -1327,6 +1368,13 @@ __device__ bool start_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
   if (!team_barrier<BS>(P, sm, bar, bar_epoch, team_size, &ctr->status, inj)) return false;
 
   if (threadIdx.x == 0) sm.bc_q = __ldcg(&ctr->qtail[0]);
+  if (learned) {
+    // the weights move to shared memory once, so each evaluation reads no global memory
+    static_assert(sizeof(PolicyDev) % 4 == 0, "word copy");
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(P.policy);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&sm.pol);
+    for (uint32_t i = threadIdx.x; i < sizeof(PolicyDev) / 4; i += BS) dst[i] = __ldg(src + i);
+  }
   __syncthreads();
   qlen = min(sm.bc_q, I.qcap);
   delta = I.dsched ? 1u << (I.dsched & 15u) : I.delta;
@@ -1350,12 +1398,12 @@ __device__ bool start_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
         if (i == 0) f = f0;
         if (i >= 1 && i <= 8 && i - 1 == sbin) f = 1.f;
         if (i == 10) f = 1.f / (float)I.n;
-        sm.feat[i] = (f - P.policy->mean[i]) * P.policy->istd[i];
+        sm.feat[i] = (f - sm.pol.mean[i]) * sm.pol.istd[i];
       }
     }
     if (warp == 0) {
       __syncwarp();
-      policy_eval_warp(P.policy, sm.feat, sm.pol_choice, lane);
+      policy_eval_warp(&sm.pol, sm.feat, sm.pol_choice, lane);
     }
     __syncthreads();
     delta = 1u << sm.pol_choice[0];
@@ -1638,7 +1686,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
         f[10] = (float)reached_total / (float)I.n;
         f[11] = ie ? (float)ii / (float)ie : 0.f;
         if (learned)
-          for (int i = 0; i < NPS_MLP_IN; ++i) sm.feat[i] = (f[i] - P.policy->mean[i]) * P.policy->istd[i];
+          for (int i = 0; i < NPS_MLP_IN; ++i) sm.feat[i] = (f[i] - sm.pol.mean[i]) * sm.pol.istd[i];
         if (I.trace && rank == 0 && it < I.trace_cap) {
           nps_trace_rec* tr = I.trace + it;
           tr->iteration = it;
@@ -1659,7 +1707,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     }
     if (learned && warp == 0) {
       __syncwarp();
-      if (sm.ok) policy_eval_warp(P.policy, sm.feat, sm.pol_choice, lane);
+      if (sm.ok) policy_eval_warp(&sm.pol, sm.feat, sm.pol_choice, lane);
     }
     __syncthreads();
     if (!sm.ok) return;
@@ -1743,16 +1791,19 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
 // bucket (the far pile's smallest distance, the policy's width).  Results are
 // exact for the reason the iteration schedule's are: the scheme is
 // label-correcting, and a vertex whose distance drops after it was taken from the
-// ring is queued again -- its mark is reset before its distance is read, the read
-// waiting for the reset by a data dependency, and the mark is set only after the
-// atomicMin that improved the distance has returned.
+// ring is queued again -- its mark is reset (an acquire) before its distance is
+// read, and the mark is set (a release) after the atomicMin that improved the
+// distance.
 //
 // Ring slots carry tags (Vyukov's bounded queue): index i may be written once its
 // slot holds tag i and read once it holds i + 1; a reader then writes i + capacity.
-// Head and tail persist across runs.  A warp claims 32 near-ring indices (or one
-// segment) only while the ring holds unclaimed entries; claims beyond the tail are
-// filled by later pushes, and those still empty when the bucket ends are released
-// by their warp, after which the tail is moved up to the head.
+// Head and tail persist across runs.  Every warp holds one claimed segment index
+// and one claimed window of 32 near-ring indices, and polls only those slots; it
+// claims again when it takes a filled segment, or the last entry of its window,
+// while it still holds that unit (so the bucket cannot end between).  Claims
+// beyond the tail are filled by later pushes; those still empty when the bucket
+// ends are handed back by their warp, and after the team barrier the tails are
+// moved up to the heads, one more barrier ahead of the next bucket.
 template <int BS>
 __device__ void solve_instance_async(const LaunchParams& P, const InstDesc& I, Smem<BS>& sm, uint32_t* bar,
                                      uint32_t& bar_epoch, uint32_t rank, uint32_t team_size, bool& inject) {
@@ -1814,6 +1865,7 @@ __device__ void solve_instance_async(const LaunchParams& P, const InstDesc& I, S
     }
     if (threadIdx.x < 8) sm.hist[threadIdx.x] = 0;
     if (threadIdx.x < 3) sm.it_acc[threadIdx.x] = 0;
+    if (threadIdx.x == 0) sm.phase_flag = 0;
     __syncthreads();
 
     const uint32_t n_static = (srclen + 31) / 32;
@@ -1837,29 +1889,28 @@ __device__ void solve_instance_async(const LaunchParams& P, const InstDesc& I, S
     bool fin = false;
     for (;;) {
       bool did = false;
-      // (1) a segment
+      // (1) a segment.  The warp always holds one claimed index of the segment ring and
+      // polls only that slot's tag (no shared counter is read while waiting); taking a
+      // filled slot claims the next index at once, so the claim's round trip overlaps
+      // the walk.  Claims beyond the tail wait for later pushes -- at most one per warp.
       if (!has_seg) {
-        uint32_t got = 0, si = 0;
-        if (lane == 0 && (int32_t)(ld_relaxed_u32(&I.rs->seg_tail) - ld_relaxed_u32(&I.rs->seg_head)) > 0) {
-          si = atomicAdd(&I.rs->seg_head, 1u);
-          got = 1;
-        }
-        if (__shfl_sync(kFull, got, 0)) {
-          has_seg = true;
-          sidx = __shfl_sync(kFull, si, 0);
-        }
+        uint32_t si = 0;
+        if (lane == 0) si = atomicAdd(&I.rs->seg_head, 1u);
+        sidx = __shfl_sync(kFull, si, 0);
+        has_seg = true;
       }
-      if (has_seg) {
+      {
         int4 sg = make_int4(0, 0, 0, 0);
-        uint32_t ready = 0;
+        uint32_t ready = 0, next = 0;
         if (lane == 0) {
           int4* slot = I.seg + (sidx & I.seg_mask);
           uint32_t* tag = reinterpret_cast<uint32_t*>(slot) + 3;
           const uint32_t tg = ld_relaxed_u32(tag);
           if (tg == sidx + 1) {
-            sg = __ldcg(slot + dep_zero(tg));  // the payload, read after the tag ...
+            sg = ld_relaxed_v4(slot + dep_zero(tg));  // the payload, read after the tag ...
             // ... and back before the slot is handed back (the store waits for it)
             st_relaxed_u32(tag + dep_zero((uint32_t)sg.x ^ (uint32_t)sg.y ^ (uint32_t)sg.z), sidx + SC);
+            next = atomicAdd(&I.rs->seg_head, 1u);
             ready = 1;
           }
         }
@@ -1868,8 +1919,8 @@ __device__ void solve_instance_async(const LaunchParams& P, const InstDesc& I, S
           sg.y = __shfl_sync(kFull, sg.y, 0);
           sg.z = __shfl_sync(kFull, sg.z, 0);
           walk_segment(I, C, sg, acc, S, lane);
+          sidx = __shfl_sync(kFull, next, 0);
           D += 1;
-          has_seg = false;
           did = true;
         }
       }
@@ -1891,15 +1942,12 @@ __device__ void solve_instance_async(const LaunchParams& P, const InstDesc& I, S
       // (3) near-ring vertices
       if (!did) {
         if (om == 0) {
-          uint32_t got = 0, b = 0;
-          if (lane == 0 && (int32_t)(ld_relaxed_u32(&I.rs->nq_tail) - ld_relaxed_u32(&I.rs->nq_head)) > 0) {
-            b = atomicAdd(&I.rs->nq_head, 32u);
-            got = 1;
-          }
-          if (__shfl_sync(kFull, got, 0)) {
-            wb = __shfl_sync(kFull, b, 0);
-            om = kFull;
-          }
+          // a new window once every slot of the last one was taken (as for segments,
+          // at most one claimed window per warp, polled slot by slot)
+          uint32_t b = 0;
+          if (lane == 0) b = atomicAdd(&I.rs->nq_head, 32u);
+          wb = __shfl_sync(kFull, b, 0);
+          om = kFull;
         }
         if (om) {
           int32_t v = -1;
@@ -1921,8 +1969,11 @@ __device__ void solve_instance_async(const LaunchParams& P, const InstDesc& I, S
           if (tm) {
             if (v >= 0) {
               // the mark is reset before the distance is read: a drop after this
-              // exchange queues v again, one before it is seen by the read
-              const uint32_t old = atomicExch(I.mark + v, 0u);
+              // exchange queues v again, one before it is seen by the read.  The reset
+              // is an acquire, paired with the producer's release: a relaxed reset
+              // followed by a dependent load still returned a stale distance on B200
+              // (a few vertices in a thousand runs came out too long)
+              const uint32_t old = atom_exch_acquire(I.mark + v, 0u);
               v += (int32_t)dep_zero(old);
             }
             process_vertex_item<BS>(I, C, sm, v, false, T_old, want_iter, acc, S, pc, lane);
@@ -1935,7 +1986,9 @@ __device__ void solve_instance_async(const LaunchParams& P, const InstDesc& I, S
         idle = 0;
         continue;
       }
-      // (4) no work at hand: publish what this warp holds, then test for the end of the bucket
+      // (4) no work at hand: publish what this warp holds, then test for the end of the
+      // bucket.  Only the CTA's warp 0 reads the shared counters; it tells the CTA's
+      // other warps through shared memory, so idle warps do not crowd those lines.
       stage_drain(I, S, C, I.qcap, &ctr->status, lane);
       uint32_t f = 0, stop = 0;
       if (lane == 0) {
@@ -1946,18 +1999,28 @@ __device__ void solve_instance_async(const LaunchParams& P, const InstDesc& I, S
           if (back) atomicSub(&ctr->pend, back);
           sm.credit[warp] = 0;
         }
-        const uint32_t sd = ld_relaxed_u32(&ctr->sdone[p % 3]);
-        if (sd >= n_static) f = ld_relaxed_u32(&ctr->pend + dep_zero(sd)) == 0;
-        if (!f) {
-          const unsigned long long now = globaltimer_ns();
-          if (idle == 0) t_idle = now;
-          if (ld_relaxed_u32(&ctr->status) != 0 || ld_relaxed_u32(P.abort_flag) != 0) {
-            stop = 1;
-          } else if (now - t_idle > P.timeout_ns || now - sm.t_start > P.run_budget_ns) {
-            atomicCAS(&ctr->status, 0u, (uint32_t)NPS_ERR_TIMEOUT);
-            atomicExch(P.abort_flag, 1u);
-            stop = 1;
+        const unsigned long long now = globaltimer_ns();
+        if (idle == 0) t_idle = now;
+        const uint32_t flag = *(volatile uint32_t*)&sm.phase_flag;
+        if (flag == p + 1) {
+          f = 1;
+        } else if (flag == 0xffffffffu) {
+          stop = 1;
+        } else if (warp == 0) {
+          if (idle >= 1) {
+            const uint32_t sd = ld_relaxed_u32(&ctr->sdone[p % 3]);
+            if (sd >= n_static) f = ld_relaxed_u32(&ctr->pend + dep_zero(sd)) == 0;
           }
+          if (!f && (idle & 15) == 15 &&
+              (ld_relaxed_u32(&ctr->status) != 0 || ld_relaxed_u32(P.abort_flag) != 0))
+            stop = 1;
+          if (f || stop) *(volatile uint32_t*)&sm.phase_flag = f ? p + 1 : 0xffffffffu;
+        }
+        if (!f && !stop && (now - t_idle > P.timeout_ns || now - sm.t_start > P.run_budget_ns)) {
+          atomicCAS(&ctr->status, 0u, (uint32_t)NPS_ERR_TIMEOUT);
+          atomicExch(P.abort_flag, 1u);
+          *(volatile uint32_t*)&sm.phase_flag = 0xffffffffu;
+          stop = 1;
         }
       }
       sdone_w = 0;
@@ -1995,18 +2058,19 @@ __device__ void solve_instance_async(const LaunchParams& P, const InstDesc& I, S
     tot.reached += acc.reached;
     tot.processed += acc.processed;
     __syncthreads();
-    if (fin && rank == 0 && threadIdx.x == 0) {
-      // move the tails up to the heads, past every claim of the bucket: no claim or
-      // push happens any more (a claim needs tail > head, and head >= tail once the
-      // pending total is zero)
+    if (!team_barrier<BS>(P, sm, bar, bar_epoch, team_size, &ctr->status, false, false,
+                          want_iter ? ctr : nullptr, p % 3))
+      return;
+    if (rank == 0 && threadIdx.x == 0) {
+      // every warp of the team has left the bucket and handed back its unfilled
+      // claims: move the tails up to the heads, past every claim, before anything
+      // is pushed again (the next bucket starts after one more barrier; the next
+      // run, after the launch ends)
       const uint32_t nh = ld_relaxed_u32(&I.rs->nq_head), nt = ld_relaxed_u32(&I.rs->nq_tail);
       if ((int32_t)(nh - nt) > 0) atomicExch(&I.rs->nq_tail, nh);
       const uint32_t sh = ld_relaxed_u32(&I.rs->seg_head), st = ld_relaxed_u32(&I.rs->seg_tail);
       if ((int32_t)(sh - st) > 0) atomicExch(&I.rs->seg_tail, sh);
     }
-    if (!team_barrier<BS>(P, sm, bar, bar_epoch, team_size, &ctr->status, false, false,
-                          want_iter ? ctr : nullptr, p % 3))
-      return;
 
     // ---- the next bucket (every CTA reads the same values)
     if (threadIdx.x == 0) {
@@ -2041,7 +2105,7 @@ __device__ void solve_instance_async(const LaunchParams& P, const InstDesc& I, S
         fv[10] = (float)reached_total / (float)I.n;
         fv[11] = ie ? (float)ii / (float)ie : 0.f;
         if (learned)
-          for (int i = 0; i < NPS_MLP_IN; ++i) sm.feat[i] = (fv[i] - P.policy->mean[i]) * P.policy->istd[i];
+          for (int i = 0; i < NPS_MLP_IN; ++i) sm.feat[i] = (fv[i] - sm.pol.mean[i]) * sm.pol.istd[i];
         if (I.trace && rank == 0 && p < I.trace_cap) {
           nps_trace_rec* tr = I.trace + p;
           tr->iteration = p;
@@ -2062,7 +2126,7 @@ __device__ void solve_instance_async(const LaunchParams& P, const InstDesc& I, S
     }
     if (learned && warp == 0) {
       __syncwarp();
-      if (sm.ok) policy_eval_warp(P.policy, sm.feat, sm.pol_choice, lane);
+      if (sm.ok) policy_eval_warp(&sm.pol, sm.feat, sm.pol_choice, lane);
     }
     __syncthreads();
     if (!sm.ok) return;
@@ -2085,6 +2149,8 @@ __device__ void solve_instance_async(const LaunchParams& P, const InstDesc& I, S
     advance = true;
     srcq = I.fq[(p - 1) & 1];
     srclen = fl;
+    // the ring counters are set before the next bucket pushes or claims anything
+    if (!team_barrier<BS>(P, sm, bar, bar_epoch, team_size, &ctr->status, false)) return;
   }
   (void)level;
 

@@ -606,6 +606,8 @@ nps_status run_single(nps_ctx* c, cudaStream_t s, const int32_t* row, const int3
   d.trace_cap = p.trace ? (uint32_t)c->trace.n : 0;
   d.vec_ok = (((uintptr_t)col | (uintptr_t)w) & 15) == 0;
   fill_thresholds(p, d);
+  d.policy = nps_policy_for(p, m);  // the learned policy only where it gains
+  if (st) st->policy_used = (uint32_t)d.policy;
   if (async) {
     d.async = 1;
     d.nq = c->nq.p;
@@ -1016,6 +1018,7 @@ extern "C" nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, co
       d.stamp_base = stamps + i;
       d.vec_ok = (((uintptr_t)x.col | (uintptr_t)x.w) & 15) == 0;
       fill_thresholds(p, d);
+      d.policy = nps_policy_for(p, x.m);
     }
     NPS_CUDA(cudaMemcpyAsync(c->b_inst.p, c->b_inst_host.data(), sizeof(InstDesc) * count, cudaMemcpyHostToDevice, s));
     NPS_CUDA(cudaMemcpyAsync(c->b_teams.p, teams.data(), sizeof(TeamDesc) * nteams, cudaMemcpyHostToDevice, s));
@@ -1087,6 +1090,7 @@ extern "C" nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, co
       per_instance[i].reached = k.reached + 1;
       per_instance[i].grid_ctas = grid;
       per_instance[i].kernel_ms = (float)((double)k.solve_ns * 1e-6);  // device time to this instance's end
+      per_instance[i].policy_used = (uint32_t)c->b_inst_host[i].policy;
     }
     if (k.status && !first_err) first_err = k.status;
   }

@@ -73,6 +73,14 @@ nps_status nps_ensure(T** p, size_t* have, size_t want, cudaStream_t s, const ch
 // so the cache is abandoned (not freed) and built again.
 unsigned long long nps_context_id(int device);
 
+// The policy a run on a graph of m edges uses: NPS_POLICY_LEARNED only from
+// p.policy_min_edges edges (0 = NPS_POLICY_MIN_EDGES, negative = any size).
+inline int32_t nps_policy_for(const nps_params& p, int64_t m) {
+  if (p.policy != NPS_POLICY_LEARNED) return p.policy;
+  const int64_t lim = p.policy_min_edges == 0 ? (int64_t)NPS_POLICY_MIN_EDGES : p.policy_min_edges;
+  return (lim > 0 && m < lim) ? (int32_t)NPS_POLICY_PLAIN : (int32_t)NPS_POLICY_LEARNED;
+}
+
 // Device copy of the learned-policy weights of `device` (null if none loaded).
 const void* nps_policy_device_weights(int device);
 

@@ -219,7 +219,7 @@ extern "C" nps_status nps_sssp_noalloc(const int32_t* d_row_ptr, const int32_t* 
   d.t2 = p.block_threshold;
   d.t3 = p.grid_threshold;
   d.delta = p.delta;
-  d.policy = p.policy;
+  d.policy = nps_policy_for(p, m);
   d.light_heavy = p.light_heavy != 0;
   d.local_rounds = p.local_rounds < 0 ? 0 : (p.local_rounds > 1024 ? 1024 : p.local_rounds);
   d.order_degree = p.order_degree < 0 ? 0 : p.order_degree;
@@ -269,6 +269,7 @@ extern "C" nps_status nps_sssp_noalloc(const int32_t* d_row_ptr, const int32_t* 
     st->reached = h.reached + 1;
     st->status = (int32_t)h.status;
     st->grid_ctas = grid;
+    st->policy_used = (uint32_t)d.policy;
   }
   switch (h.status) {
     case NPS_OK: return NPS_OK;

@@ -42,9 +42,10 @@ def median_ms(dg, p, reps=5):
 
 def learned_params(plain):
     """The learned configuration: the plain one with the policy deciding widths and
-    levels (no light/heavy split and no degree ordering, as in the teacher runs)."""
+    levels (no light/heavy split and no degree ordering, as in the teacher runs), on
+    graphs of every size (the library's minimum graph size for the policy is off)."""
     return dataclasses.replace(plain, policy=nps.POLICY_LEARNED, light_heavy=False, order_degree=0,
-                               delta_schedule=0)
+                               delta_schedule=0, policy_min_edges=-1)
 
 
 def main():

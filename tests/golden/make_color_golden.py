@@ -2,11 +2,11 @@
 """Golden colors from the reference's own graph-coloring program.
 
 Runs oracle/_ref/gpu-graph-color -- the reference's gpu-graph-color built from its
-sources (apps/graph-color/src/gpu) by oracle/Makefile -- with `-s 0 -d` on the three
+sources (apps/graph-color/src/gpu) by oracle/Makefile -- with `-s 0` on the three
 golden reader files and on generated graphs written as DIMACS9, and records every
-vertex's color as the program prints it ("Node i: c", from gclr_nopruning_gpu():
-one gclr_bitmap_kernel launch per color, graph_color_wrapper.cu:113-130,
-graph_color_kernel.cu:14-35).  It needs a GPU; the output is committed as
+vertex's color (gclr_nopruning_gpu(): one gclr_bitmap_kernel launch per color,
+graph_color_wrapper.cu:113-130, graph_color_kernel.cu:14-35; written out by the hook
+of oracle/ref_gclr_hook.cpp).  It needs a GPU; the output is committed as
 tests/golden/color_reference.json and checked against the oracle on CPU by
 tests/test_color_cpu.py.
 
@@ -37,18 +37,11 @@ GENERATED = {
 
 
 def run_reference(path, fmt):
-    r = subprocess.run([BIN, "-s", "0", "-d", "-f", str(fmt), "-i", path], capture_output=True, text=True,
-                       timeout=600, check=True)
-    colors = {}
-    for line in r.stdout.splitlines():
-        if line.startswith("Node "):
-            k, c = line[5:].split(":")
-            colors[int(k) - 1] = int(c)
-    n = max(colors) + 1 if colors else 0
-    out = np.zeros(n, dtype=np.int32)
-    for k, c in colors.items():
-        out[k] = c
-    return out
+    with tempfile.TemporaryDirectory() as td:
+        out = os.path.join(td, "colors.bin")
+        subprocess.run([BIN, "-s", "0", "-f", str(fmt), "-i", path], capture_output=True, text=True, timeout=600,
+                       check=True, env=dict(os.environ, NPS_REF_COLORS=out))
+        return np.fromfile(out, dtype=np.int32)
 
 
 def fnv1a(a):
@@ -64,7 +57,7 @@ def main():
     a = ap.parse_args()
     sys.path.insert(0, ROOT)
     nps = importlib.import_module("nested-parallelism_b200")
-    res = {"generator": "tests/golden/make_color_golden.py", "program": "gpu-graph-color -s 0 -d", "graphs": {}}
+    res = {"generator": "tests/golden/make_color_golden.py", "program": "gpu-graph-color -s 0", "graphs": {}}
     for name, fmt in READERS:
         c = run_reference(os.path.join(HERE, name), fmt)
         res["graphs"][name] = {"format": fmt, "n": int(c.size), "max_color": int(c.max()), "colors": c.tolist()}

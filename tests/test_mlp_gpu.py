@@ -89,7 +89,7 @@ def test_fused_policy_takes_the_oracle_decisions(nps, pol, cuda_device):
     w.mean[:] = 1.0
     w.istd[:] = 0.5
     pol.load_into_kernel(w, 0)
-    p = nps.Params(policy=nps.POLICY_LEARNED, delta=16, trace=True, light_heavy=False)
+    p = nps.Params(policy=nps.POLICY_LEARNED, delta=16, trace=True, light_heavy=False, policy_min_edges=-1)
     d, st = nps.sssp(g, g.source, p)
     tr = nps.trace_read(0)  # the trace of the most recent call
     assert np.array_equal(d, nps.sssp(g, g.source, nps.Params())[0])  # exact regardless of the policy
@@ -107,7 +107,7 @@ def test_fused_policy_widths_follow_the_oracle(nps, pol, cuda_device):
     w = pol.MLPWeights.init(17)
     w.b2[:11] = np.linspace(0.0, 0.5, 11)  # spread the width logits
     pol.load_into_kernel(w, 0)
-    p = nps.Params(policy=nps.POLICY_LEARNED, trace=True, light_heavy=False)
+    p = nps.Params(policy=nps.POLICY_LEARNED, trace=True, light_heavy=False, policy_min_edges=-1)
     d, st = nps.sssp(g, g.source, p)
     tr = nps.trace_read(0)
 

@@ -70,3 +70,29 @@ def test_reference_program_on_a_power_law_graph(nps, oracle, cuda_device, tmp_pa
     h = nps.readInputDIMACS9(path)
     got = _run(BINS[level], 0, path, tmp_path)
     assert np.array_equal(got, oracle.sssp_heap(h.row_ptr, h.col, h.w, h.source))
+
+
+OWN = {lv: os.path.join(REF, f"gpu-sssp-ref-l{lv}") for lv in (0, 1, 2)}
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not all(os.path.exists(b) for b in OWN.values()),
+                    reason="the reference's gpu-sssp was not built (needs the reference sources)")
+@pytest.mark.parametrize("level", [0, 1, 2])
+def test_library_equals_the_reference_gpu_kernels_on_the_uniform_graph(nps, oracle, cuda_device, tmp_path, level):
+    """The reference's own consolidation kernels (consolidate_{warp,block,grid}_dp_kernel with their
+    dynamic-parallelism children, sssp_kernel.cu:330-541, driven by sssp_np_consolidate_gpu(),
+    sssp_wrapper.cu:475-546) on the CPU-runnable configuration: 16,384 vertices, 131,072 uniform
+    edges, weights in [1, 100], source 0.  At this size every per-warp (256-slot) and per-block
+    (2048-slot) slice of the reference's 10.24 M-entry buffer lies inside it (at most 86 blocks of
+    192 threads), so the kernels stay in bounds.  The library's distances, the reference kernels'
+    and the CPU oracle's must all agree."""
+    g = nps.gen_uniform(16384, 131072, 100, 1)
+    path = str(tmp_path / "uniform16k.gr")
+    nps.writeDIMACS9(path, g)
+    h = nps.readInputDIMACS9(path)
+    want = oracle.sssp_heap(h.row_ptr, h.col, h.w, h.source)
+    ref = _run(OWN[level], 0, path, tmp_path)
+    mine, _ = nps.sssp(h, h.source, nps.Params(level=level))
+    assert np.array_equal(mine, want)
+    assert np.array_equal(ref, want), f"reference kernels: {(ref != want).sum()} mismatches against the oracle"
