@@ -44,7 +44,8 @@
  *                      or colored c.  Both block v whatever the order, so v ends with
  *                      1 + the largest color of its smaller out-neighbours; in id order
  *                      those are final when v is reached.  The reference has no CPU
- *                      version of this path (parity unpinned: see the test header).
+ *                      version of this path; the result is pinned to its GPU program's
+ *                      colors (tests/golden/color_reference.json).
  *
  *   oracle_gen_rmat    the benchmark's seeded R-MAT input (a restatement of this
  *                      library's own generator, so the reference's CPU path can be
