@@ -965,38 +965,39 @@ def bench_color(a, nps, ws, rank, local, desc):
 # with the oracle's restatement of the generator (identical arrays, checked by
 # tests/test_oracle_cpu.py), so no CPU process ever loads the library.
 
-def _rmat_cpu_worker(scale, ef, seed, reps, use_ref, q, go, timeout_s):
-    """One host process: build R-MAT (scale, ef, seed), report ready, wait for `go`,
-    then run `reps` single-source searches by the reference's SSSP_CPU (oracle/_ref)
-    or, without it, the oracle's restatement; report the distance hash and times."""
+def _rmat_cpu_worker(scale, ef, seeds, use_ref, q, go, timeout_s):
+    """One host process: build the R-MAT (scale, ef) graphs of `seeds` (each distinct
+    seed once), report ready, wait for `go`, then run one single-source search per entry
+    of `seeds`, in order, by the reference's SSSP_CPU (oracle/_ref) or, without it, the
+    oracle's restatement; report each search's distance hash and time."""
     os.environ["OMP_NUM_THREADS"] = "1"  # one core per process
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     try:
-        row, col, w, src = oracle.gen_rmat(scale, ef, seed)
-        q.put(("ready", seed))
+        graphs = {sd: oracle.gen_rmat(scale, ef, sd) for sd in dict.fromkeys(seeds)}
+        q.put(("ready", seeds[0]))
         if not go.wait(timeout_s):
-            q.put(("error", seed, "start signal never came"))
+            q.put(("error", seeds[0], "start signal never came"))
             return
-        times, d = [], None
-        for _ in range(reps):
+        for sd in seeds:
+            row, col, w, src = graphs[sd]
             if use_ref:
                 d, t = oracle.ref_sssp_cpu(row, col, w, src)
             else:
                 d, t = oracle.timed(oracle.sssp_heap, row, col, w, src)
-            times.append(t)
-        n_r, m_r = oracle.reached(row, d)
-        q.put(("done", seed, oracle.fnv1a(d), times, n_r, m_r, src, int(row.shape[0] - 1), int(col.shape[0])))
+            n_r, m_r = oracle.reached(row, d)
+            q.put(("done", sd, oracle.fnv1a(d), t, n_r, m_r, src, int(row.shape[0] - 1), int(col.shape[0])))
     except Exception as e:  # reported to the parent, which fails loudly
-        q.put(("error", seed, repr(e)))
+        q.put(("error", seeds[0], repr(e)))
 
 
 class CpuSearches:
-    """Spawned processes, one per (seed, repetitions): each builds its graph, and all
-    start their searches together once every graph is built (synchronized) or as
-    soon as their own is (not synchronized)."""
+    """Spawned processes, each with a list of seeds: every process builds its graphs,
+    then all start their searches together once every graph is built (synchronized)
+    or as soon as their own are (not synchronized).  `runs` lists every search's
+    result; `results` keeps the first per seed."""
 
-    def __init__(self, scale, ef, seed_reps, use_ref, synchronized, timeout_s=1800):
+    def __init__(self, scale, ef, seed_lists, use_ref, synchronized, timeout_s=1800):
         import multiprocessing as mp
         ctx = mp.get_context("spawn")
         self.q, self.go = ctx.Queue(), ctx.Event()
@@ -1004,12 +1005,14 @@ class CpuSearches:
         if not synchronized:
             self.go.set()
         self.procs = [ctx.Process(target=_rmat_cpu_worker,
-                                  args=(scale, ef, sd, r, use_ref, self.q, self.go, timeout_s), daemon=True)
-                      for sd, r in seed_reps]
+                                  args=(scale, ef, list(sl), use_ref, self.q, self.go, timeout_s), daemon=True)
+                      for sl in seed_lists if sl]
+        self.expected = sum(len(sl) for sl in seed_lists)
         for pr in self.procs:
             pr.start()
         self.timeout_s = timeout_s
         self.wall = None
+        self.runs = []
         self.results = {}
 
     def _get(self):
@@ -1044,14 +1047,29 @@ class CpuSearches:
         return self.results
 
     def collect(self):
-        while len(self.results) < len(self.procs):
+        while len(self.runs) < self.expected:
             msg = self._get()
             if msg[0] == "done":
-                _, seed, h, times, n_r, m_r, src, n, m = msg
-                self.results[seed] = dict(fnv=h, times=times, n_r=n_r, m_r=m_r, source=src, n=n, m=m)
+                _, seed, h, t, n_r, m_r, src, n, m = msg
+                r = dict(seed=seed, fnv=h, seconds=t, n_r=n_r, m_r=m_r, source=src, n=n, m=m)
+                self.runs.append(r)
+                self.results.setdefault(seed, r)
         for pr in self.procs:
             pr.join(timeout=60)
         return self.results
+
+
+def _cpu_processes(scale, ef, wanted):
+    """Processes to run at once: at most `wanted`, the host's cores, and what 60 % of
+    the available memory holds at the generator's peak (about 40 bytes per edge)."""
+    cores = os.cpu_count() or 1
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except Exception:
+        avail = 64 << 30
+    per_proc = (ef << scale) * 40 + (256 << 20)
+    return max(1, min(wanted, cores, int(avail * 0.6 // per_proc)))
 
 
 def _cpu_use_ref():
@@ -1071,53 +1089,50 @@ def rmat_eval_config(wl, desc, seeds, per_seed):
 
 
 def reference_rmat_eval(a, wl, desc):
-    """--impl reference on the evaluation workload: the reference's SSSP_CPU on the
-    host cores, one process per graph, all searches started together; a step = one
-    SSSP of each graph (the arm's K steps are K searches per graph)."""
+    """--impl reference on the evaluation workload: the reference's SSSP_CPU on the host
+    cores.  Each of the K steps is one full SSSP of one evaluation graph (seeds in turn);
+    the steps run in parallel processes, one core each, all started together after every
+    graph is built, and the value is the reached edges of all K searches over the wall time."""
     _, w, _ = WORKLOADS[wl]
-    seeds = a.seeds or w["seeds"]
+    seeds = list(a.seeds or w["seeds"])
     use_ref = _cpu_use_ref()
-    cores = os.cpu_count() or 1
-    try:
-        import psutil
-        avail = psutil.virtual_memory().available
-    except Exception:
-        avail = 64 << 30
-    per_proc = (w["edge_factor"] << w["scale"]) * 40 + (256 << 20)  # generator peak, bytes
-    procs = max(1, min(len(seeds), cores, int(avail * 0.6 // per_proc)))
-    seeds = list(seeds)[:procs] if procs < len(seeds) else list(seeds)
-    cs = CpuSearches(w["scale"], w["edge_factor"], [(sd, a.steps) for sd in seeds], use_ref, synchronized=True)
+    steps = [seeds[i % len(seeds)] for i in range(a.steps)]
+    procs = _cpu_processes(w["scale"], w["edge_factor"], len(steps))
+    lists = [steps[j::procs] for j in range(procs)]
+    cs = CpuSearches(w["scale"], w["edge_factor"], lists, use_ref, synchronized=True)
     res = cs.start()
     wall = cs.wall
-    total_edges = a.steps * sum(res[sd]["m_r"] for sd in seeds)
+    total_edges = sum(r["m_r"] for r in cs.runs)
     value = total_edges / wall / 1e9
+    used = sorted(res)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": a.gpus,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * wall / a.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-        "data": "synthetic", "config": rmat_eval_config(wl, desc, seeds, res),
-        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": len(seeds),
+        "data": "synthetic", "config": rmat_eval_config(wl, desc, used, res),
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": procs,
                          "kind": "reference" if use_ref else "port",
-                         "sample": f"every step: one full SSSP of each of the {len(seeds)} graphs, one process "
-                                   "(one core) per graph, all started together; "
+                         "sample": f"{a.steps} full SSSPs, one per step, the evaluation graphs in turn, {procs} "
+                                   "processes (one core each) started together; "
                                    + ("the reference's SSSP_CPU (apps/sssp/src/cpu/sssp.cpp) built from its "
                                       "sources" if use_ref else "the oracle's restatement of SSSP_CPU")},
         "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "per_seed_seconds": {str(sd): res[sd]["times"] for sd in seeds},
-        "warmup_note": "warm-up = every process builds its graph and loads the reference code before the "
+        "seconds_per_search": [round(r["seconds"], 3) for r in cs.runs],
+        "warmup_note": "warm-up = every process builds its graphs and loads the reference code before the "
                        "timed searches start",
     }
     if use_ref:
         # the reference's other CPU path, usssp_cpu (apps/sssp/src/cpu/sssp_kernel.cpp): an OpenMP frontier
         # sweep on every host thread, on the first graph; its concurrent updates race, so it is reported with
-        # its mismatch count and never used as a result
+        # whether it matched Dijkstra (distance hash) and never used as a result
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle
-        row, col, wt, src = oracle.gen_rmat(w["scale"], w["edge_factor"], seeds[0])
-        d0, _ = oracle.ref_sssp_cpu(row, col, wt, src)
+        cores = os.cpu_count() or 1
+        sd = used[0]
+        row, col, wt, src = oracle.gen_rmat(w["scale"], w["edge_factor"], sd)
         du, tu = oracle.ref_usssp_cpu(row, col, wt, src, threads=cores)
-        line["usssp_cpu"] = {"value": res[seeds[0]]["m_r"] / tu / 1e9, "unit": "GTEPS", "threads": cores,
-                             "seconds": tu, "seed": seeds[0], "mismatches_vs_dijkstra": int((du != d0).sum()),
+        line["usssp_cpu"] = {"value": res[sd]["m_r"] / tu / 1e9, "unit": "GTEPS", "threads": cores,
+                             "seconds": tu, "seed": sd, "equal_to_dijkstra": oracle.fnv1a(du) == res[sd]["fnv"],
                              "exact": False, "note": "racy: concurrent unsynchronised updates (non-exact by design)"}
     return line
 
@@ -1131,7 +1146,8 @@ def bench_rmat_eval(a, ws, rank, local, wl, desc):
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         # started before the first CUDA call (spawned processes, no library loaded)
-        cpu = CpuSearches(w["scale"], w["edge_factor"], [(sd, 1) for sd in seeds], _cpu_use_ref(),
+        procs = _cpu_processes(w["scale"], w["edge_factor"], len(seeds))
+        cpu = CpuSearches(w["scale"], w["edge_factor"], [seeds[j::procs] for j in range(procs)], _cpu_use_ref(),
                           synchronized=False)
     nps = importlib.import_module("nested-parallelism_b200")
     import torch
@@ -1281,7 +1297,7 @@ def bench_rmat_eval(a, ws, rank, local, wl, desc):
         fn = nps.fnv1a
         exact = {str(sd): bool(res[sd]["fnv"] == fn(d_head[j]) and res[sd]["fnv"] == fn(d_plain[j]))
                  for j, sd in enumerate(seeds)}
-        secs = [res[sd]["times"][0] for sd in seeds]
+        secs = [res[sd]["seconds"] for sd in seeds]
         use_ref = _cpu_use_ref()
         cpu_line = {"value": float(np.mean([m / t / 1e9 for m, t in zip(mr, secs)])), "unit": "GTEPS", "cores": 1,
                     "kind": "reference" if use_ref else "port",
