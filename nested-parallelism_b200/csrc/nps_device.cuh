@@ -87,7 +87,7 @@ struct __align__(128) Counters {
   unsigned long long it_edges[3];
   unsigned long long it_impr[3];
   uint32_t it_reached[3];
-  uint32_t pad1[3];
+  uint32_t it_early[3];  // rows sorted into the grid-tier list when pushed (part of the next frontier)
   unsigned long long prof[9];   // NPS_PROFILE builds: SM cycles per phase, summed over warps
   unsigned long long solve_ns;  // end of this instance's solve, from its team CTA 0's start
   // asynchronous buckets: ring units (near-ring vertices and segments) pushed and not yet
@@ -375,12 +375,63 @@ struct IterCtx {
   int32_t order_deg;     // improved vertices below this degree join the near queue at any distance
   bool ring;             // asynchronous bucket: near pushes go to the near ring, grid-tier rows
                          // to the segment ring (qn, heavy and the item tables are unused)
+  bool early;            // near pushes of at least t_grid edges join this iteration's grid-tier
+                         // list when their staging buffer is flushed (walked next iteration)
+  bool want_hist;        // policy features or trace: count the degrees of those rows
 };
 
 // Whether an edge of weight w is relaxed by a pass over light (heavy = false)
 // or heavy (heavy = true) edges.
 __device__ __forceinline__ bool edge_in_pass(const IterCtx& C, uint32_t w, bool heavy) {
   return C.split == 0u || (heavy ? w >= C.split : w < C.split);
+}
+
+// Append the lanes' rows with `g` set ({s, e, vtag}) to this iteration's grid-tier
+// list.  One atomicAdd per warp reserves list slots and chunk offsets for all of
+// them (a per-row atomic on this one counter serialises large frontiers); within
+// the warp, slots and offsets follow lane order, so offsets still grow with the
+// slot across the list.  The entry holds the first chunk of every work item that
+// starts inside it; the warp then writes those item starts together, one row at a
+// time.  Warp-collective.
+__device__ __forceinline__ void grid_append(const InstDesc& I, const IterCtx& C, bool g, int32_t s, int32_t e,
+                                            int32_t vtag, int lane) {
+  const uint32_t gmask = __ballot_sync(kFull, g);
+  if (!gmask) return;
+  uint32_t slot = 0xffffffffu, b0 = 0, b1 = 0;  // list slot and work items [b0, b1) starting in it
+  const uint32_t nch = g ? row_chunks(s, e) : 0u;
+  uint32_t incl = nch;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const uint32_t wtot = __shfl_sync(kFull, incl, 31);
+  const int leader = __ffs(gmask) - 1;
+  unsigned long long old = 0;
+  if (lane == leader) old = atomicAdd(C.heavy_ctr, ((unsigned long long)__popc(gmask) << kHeavyShift) | wtot);
+  old = __shfl_sync(kFull, old, leader);
+  const uint32_t off = (uint32_t)(old & kHeavyMask) + (incl - nch);
+  if (g) {
+    slot = (uint32_t)(old >> kHeavyShift) + (uint32_t)__popc(gmask & lanemask_lt());
+    if (slot < C.hcap) {
+      C.heavy[slot] = make_int4(s, e, vtag, (int32_t)off);
+      const uint32_t sh = I.item_shift;
+      b0 = (off + (1u << sh) - 1) >> sh;
+      b1 = ((off + nch - 1) >> sh) + 1;
+      if (b1 > I.icap) atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_CAPACITY);
+    } else {
+      atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_CAPACITY);
+    }
+  }
+  uint32_t wb = __ballot_sync(kFull, b1 > b0);
+  while (wb) {
+    const int src_lane = __ffs(wb) - 1;
+    wb &= wb - 1;
+    const uint32_t rs = __shfl_sync(kFull, slot, src_lane);
+    const uint32_t r0 = __shfl_sync(kFull, b0, src_lane);
+    const uint32_t r1 = min(__shfl_sync(kFull, b1, src_lane), I.icap);
+    for (uint32_t b = r0 + lane; b < r1; b += 32) C.hitem[b] = (int32_t)rs;
+  }
 }
 
 // Thread-local accumulators, reduced per CTA.
@@ -530,6 +581,8 @@ struct Stage {
   uint32_t scnt;
   uint32_t fmin;   // per lane: smallest distance pushed into the far pile (ring mode)
   uint32_t* credit;  // ring mode: pending-total credits this warp holds (shared memory, lane 0)
+  uint32_t* hnext;   // push-time sorting: degree histogram of the rows sorted (next iteration's)
+  uint32_t* enext;   // push-time sorting: rows sorted in this iteration
 };
 
 // Move the first `nflush` staged entries to q and shift the rest down.
@@ -641,12 +694,98 @@ __device__ __forceinline__ void stage_k(int32_t* buf, uint32_t& cnt, const bool 
   }
 }
 
+// Near-queue flush with push-time sorting: the first `nflush` staged vertices are
+// looked up in row_ptr (32 at a time, one per lane); rows of at least t_grid edges
+// join this iteration's grid-tier list, so the next iteration walks them (sorted
+// when they are taken from the queue instead, they would wait one iteration more),
+// and the others go to the near queue with one atomicAdd on its tail.  The rest of
+// the buffer moves down.  Warp-collective.
+__device__ __forceinline__ void sort_flush(const InstDesc& I, const IterCtx& C, Stage& S, uint32_t nflush,
+                                               int lane) {
+  __syncwarp();
+  uint32_t kept = 0, nsorted = 0;
+  const uint32_t lt = lanemask_lt();
+  for (uint32_t g0 = 0; g0 < nflush; g0 += 32) {
+    const uint32_t i = g0 + lane;
+    const int32_t v = i < nflush ? S.nbuf[i] : -1;
+    int32_t s = 0, e = 0;
+    if (v >= 0) {
+      s = ld_index(I.row_ptr + v);
+      e = ld_index(I.row_ptr + v + 1);
+      if (s < 0 || e < s || e > I.m) {  // malformed CSR row: record; the queue entry reports it again
+        atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_FORMAT);
+        s = e = 0;
+      }
+    }
+    const bool g = v >= 0 && e > s && e - s >= C.t_grid;
+    grid_append(I, C, g, s, e, v, lane);
+    if (C.want_hist) {
+      const int bin = g ? deg_bin(e - s) : 8;
+      const uint32_t grp = __match_any_sync(kFull, bin);
+      if (g && lane == __ffs(grp) - 1) atomicAdd(&S.hnext[bin], (uint32_t)__popc(grp));
+    }
+    nsorted += __popc(__ballot_sync(kFull, g));
+    const bool keep = v >= 0 && !g;
+    const uint32_t b = __ballot_sync(kFull, keep);
+    __syncwarp();  // every lane has read its entry of this group
+    // compaction in place: kept + rank <= g0 + lane, so no entry of a later group is overwritten
+    if (keep) S.nbuf[kept + __popc(b & lt)] = v;
+    kept += __popc(b);
+  }
+  __syncwarp();
+  if (C.want_hist && lane == 0 && nsorted) atomicAdd(S.enext, nsorted);
+  if (kept) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(C.qn_tail, kept);
+    base = __shfl_sync(kFull, base, 0);
+    for (uint32_t i = lane; i < kept; i += 32) {
+      if (base + i < I.qcap) C.qn[base + i] = S.nbuf[i];
+      else atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_CAPACITY);
+    }
+  }
+  const uint32_t rem = S.ncnt - nflush;
+  int32_t t = 0;
+  if ((uint32_t)lane < rem) t = S.nbuf[nflush + lane];
+  __syncwarp();
+  if ((uint32_t)lane < rem) S.nbuf[lane] = t;
+  __syncwarp();
+  S.ncnt = rem;
+}
+
+// Stage near-queue pushes (four per lane) and flush once kFlushAt are waiting.
+__device__ __forceinline__ void stage_near(const InstDesc& I, const IterCtx& C, Stage& S, const bool (&f)[4],
+                                           const int32_t (&v)[4], int lane) {
+  if (!C.early) {
+    stage_k<4>(S.nbuf, S.ncnt, f, v, C.qn, C.qn_tail, I.qcap, &I.ctr->status, lane, C.ring ? &I : nullptr,
+               S.credit);
+    return;
+  }
+  uint32_t b[4];
+  uint32_t tot = 0;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    b[j] = __ballot_sync(kFull, f[j]);
+    tot += __popc(b[j]);
+  }
+  if (tot == 0) return;
+  const uint32_t lt = lanemask_lt();
+  uint32_t base = S.ncnt;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    if (f[j]) S.nbuf[base + __popc(b[j] & lt)] = v[j];
+    base += __popc(b[j]);
+  }
+  S.ncnt += tot;
+  if (S.ncnt >= (uint32_t)kFlushAt) sort_flush(I, C, S, S.ncnt & ~31u, lane);
+}
+
 // End of an iteration: everything staged goes to the global queues (near pushes to
 // the near ring in ring mode).
 __device__ __forceinline__ void stage_drain(const InstDesc& I, Stage& S, const IterCtx& C, uint32_t qcap,
                                             uint32_t* status, int lane) {
   if (S.ncnt) {
     if (C.ring) ring_flush(I, S.nbuf, S.ncnt, S.ncnt, lane, S.credit);
+    else if (C.early) sort_flush(I, C, S, S.ncnt, lane);
     else stage_flush(S.nbuf, S.ncnt, S.ncnt, C.qn, C.qn_tail, qcap, status, lane);
   }
   if (S.fcnt) stage_flush(S.fbuf, S.fcnt, S.fcnt, C.fp, C.fp_tail, qcap, status, lane);
@@ -666,8 +805,7 @@ __device__ __forceinline__ void relax_and_push(const InstDesc& I, const IterCtx&
     const bool fn[4] = {pn[h], pn[h + 1], pn[h + 2], pn[h + 3]};
     const bool ff[4] = {pf[h], pf[h + 1], pf[h + 2], pf[h + 3]};
     const int32_t vv[4] = {v[h], v[h + 1], v[h + 2], v[h + 3]};
-    stage_k<4>(S.nbuf, S.ncnt, fn, vv, C.qn, C.qn_tail, I.qcap, &I.ctr->status, lane, C.ring ? &I : nullptr,
-               S.credit);
+    stage_near(I, C, S, fn, vv, lane);
     stage_k<4>(S.fbuf, S.fcnt, ff, vv, C.fp, C.fp_tail, I.qcap, &I.ctr->status, lane);
   }
   if (C.ring) {
@@ -727,7 +865,8 @@ struct Smem {
   float feat[NPS_MLP_IN];
   int32_t pol_choice[2];
   PolicyDev pol;               // the policy's weights, copied once per solve (learned runs only)
-  uint32_t it_acc[3];          // this CTA's edges, improvements, first reaches in the iteration
+  uint32_t it_acc[4];          // this CTA's edges, improvements, first reaches, rows sorted at push
+  uint32_t hist_next[8];       // degree histogram of rows sorted at push (the next iteration's frontier)
   uint32_t credit[BS / 32];    // ring mode: pending-total credits held per warp
   uint32_t phase_flag;         // ring mode: set by the CTA's warp 0 when the bucket ends (p + 1) or
                                // must stop (0xffffffff); the CTA's other warps read it, not global memory
@@ -762,6 +901,7 @@ __device__ __forceinline__ bool team_barrier(const LaunchParams& P, Smem<BS>& sm
       if (sm.it_acc[0]) atomicAdd(&flush->it_edges[flush_slot], (unsigned long long)sm.it_acc[0]);
       if (sm.it_acc[1]) atomicAdd(&flush->it_impr[flush_slot], (unsigned long long)sm.it_acc[1]);
       if (sm.it_acc[2]) atomicAdd(&flush->it_reached[flush_slot], sm.it_acc[2]);
+      if (sm.it_acc[3]) atomicAdd(&flush->it_early[flush_slot], sm.it_acc[3]);
       for (int b = 0; b < 8; ++b)
         if (sm.hist[b]) atomicAdd(&flush->hist[flush_slot][b], sm.hist[b]);
     }
@@ -1030,7 +1170,7 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
   // lists then hold each vertex at most once per iteration, which bounds their size.
   bool wtier = local ? deg >= C.t_warp : (deg >= C.t_warp && deg < C.t_block);
   const bool btier = !local && deg >= C.t_block && deg < C.t_grid;
-  const bool gtier = !local && deg >= C.t_grid && deg > 0;
+  bool gtier = !local && deg >= C.t_grid && deg > 0;
   if (btier) {
     // slot and chunk offset from one atomic, so offsets increase with the slot
     const unsigned long long old = atomicAdd(&sm.blk_ctr, (1ull << 32) | row_chunks(s, e));
@@ -1041,50 +1181,10 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
   if (C.ring) {
     if (!push_segments(I, gtier, s, e, vtag, lane, S.credit)) wtier = wtier || gtier;  // ring half full: walk it here
   } else {
-    uint32_t slot = 0xffffffffu, b0 = 0, b1 = 0;  // list slot and work items [b0, b1) starting in it
-    // one atomicAdd per warp reserves list slots and chunk offsets for all of its
-    // grid-tier rows (a per-row atomic on this one counter serialises large frontiers);
-    // within the warp, slots and offsets follow lane order, so offsets still grow
-    // with the slot across the list
-    const uint32_t gmask = __ballot_sync(kFull, gtier);
-    if (gmask) {
-      const uint32_t nch = gtier ? row_chunks(s, e) : 0u;
-      uint32_t incl = nch;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(kFull, incl, o);
-        if (lane >= o) incl += t;
-      }
-      const uint32_t wtot = __shfl_sync(kFull, incl, 31);
-      const int leader = __ffs(gmask) - 1;
-      unsigned long long old = 0;
-      if (lane == leader) old = atomicAdd(C.heavy_ctr, ((unsigned long long)__popc(gmask) << kHeavyShift) | wtot);
-      old = __shfl_sync(kFull, old, leader);
-      const uint32_t off = (uint32_t)(old & kHeavyMask) + (incl - nch);
-      slot = (uint32_t)(old >> kHeavyShift) + (uint32_t)__popc(gmask & lanemask_lt());
-      if (!gtier) {
-        slot = 0xffffffffu;
-      } else if (slot < C.hcap) {
-        C.heavy[slot] = make_int4(s, e, vtag, (int32_t)off);
-        const uint32_t sh = I.item_shift;
-        b0 = (off + (1u << sh) - 1) >> sh;
-        b1 = ((off + nch - 1) >> sh) + 1;
-        if (b1 > I.icap) atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_CAPACITY);
-      } else {
-        atomicCAS(&I.ctr->status, 0u, (uint32_t)NPS_ERR_CAPACITY);
-      }
-    }
-    // the entry holds the first chunk of every work item that starts inside it; the
-    // warp writes those item starts together, one appended row at a time
-    uint32_t wb = __ballot_sync(kFull, b1 > b0);
-    while (wb) {
-      const int src_lane = __ffs(wb) - 1;
-      wb &= wb - 1;
-      const uint32_t rs = __shfl_sync(kFull, slot, src_lane);
-      const uint32_t r0 = __shfl_sync(kFull, b0, src_lane);
-      const uint32_t r1 = min(__shfl_sync(kFull, b1, src_lane), I.icap);
-      for (uint32_t b = r0 + lane; b < r1; b += 32) C.hitem[b] = (int32_t)rs;
-    }
+    // with push-time sorting a row may already be in this iteration's list (pushed and
+    // sorted earlier in it): the near stamp decides which of the two appends it
+    if (C.early && gtier) gtier = atomicExch(I.mark + v, C.snear) != C.snear;
+    grid_append(I, C, gtier, s, e, vtag, lane);
   }
 
   NPS_LAP(pc, 1);
@@ -1448,6 +1548,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
   uint32_t buckets = 0;
   uint32_t reached_total = 1;
   const uint32_t hhalf = I.hcap / 2;
+  if (threadIdx.x < 8) sm.hist_next[threadIdx.x] = 0;
 
   for (;;) {
     // ---- iteration set-up (identical in every CTA)
@@ -1475,6 +1576,9 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     C.order_deg = I.order_degree;
     C.ring = false;  // queues and lists of the iteration schedule
     level_thresholds(level, I.t1, I.t2, I.t3, C.t_warp, C.t_block, C.t_grid);
+    // push-time sorting into the grid-tier list: plain iterations at the grid level
+    C.early = !heavy_it && C.sq == nullptr && C.t_grid != 0x7fffffff;
+    C.want_hist = want_iter;
     const int4* Hprev = I.heavy + ((it & 1) ? 0 : hhalf);
     const int32_t* Hitem = I.hitem + ((it & 1) ? 0 : I.icap);
 
@@ -1492,11 +1596,16 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
           ctr->it_edges[sl] = 0;
           ctr->it_impr[sl] = 0;
           ctr->it_reached[sl] = 0;
+          ctr->it_early[sl] = 0;
         }
       }
     }
-    if (threadIdx.x < 8) sm.hist[threadIdx.x] = 0;
-    if (threadIdx.x < 3) sm.it_acc[threadIdx.x] = 0;
+    if (threadIdx.x < 8) {
+      // rows sorted at push in the last iteration belong to this iteration's frontier
+      sm.hist[threadIdx.x] = sm.hist_next[threadIdx.x];
+      sm.hist_next[threadIdx.x] = 0;
+    }
+    if (threadIdx.x < 4) sm.it_acc[threadIdx.x] = 0;
     __syncthreads();
 
     const int32_t* srcq = advance ? I.fq[ep & 1] : (heavy_it ? I.sq[hg & 1] : I.q[it & 1]);
@@ -1518,6 +1627,8 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     S.scnt = 0;
     S.fmin = 0xffffffffu;
     S.credit = nullptr;  // ring mode only
+    S.hnext = sm.hist_next;
+    S.enext = &sm.it_acc[3];
 
     // ---- work loop: heavy chunk items, then vertex items.  With no more items than
     // warps, warp w takes item w (no atomics); otherwise items come from striped
@@ -1651,12 +1762,13 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
       const uint32_t st1 = ld_relaxed_u32(&ctr->status);
       uint32_t hb[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       unsigned long long ie = 0, ii = 0;
-      uint32_t ir = 0;
+      uint32_t ir = 0, ea = 0;
       if (want_iter) {
         for (int b = 0; b < 8; ++b) hb[b] = __ldcg(&ctr->hist[sl][b]);
         ie = __ldcg(&ctr->it_edges[sl]);
         ii = __ldcg(&ctr->it_impr[sl]);
         ir = __ldcg(&ctr->it_reached[sl]);
+        ea = __ldcg(&ctr->it_early[sl]);
       }
       sm.bc_q = q1;
       sm.bc_h = h1;
@@ -1680,7 +1792,8 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
         for (int b = 0; b < 8; ++b) hs += (float)hb[b];
         const float inv = hs > 0.f ? 1.f / hs : 0.f;
         float f[NPS_MLP_IN];
-        f[0] = log2f(1.f + (float)(adv0 ? fl0 : qn0));
+        // the next frontier: its queue and the rows sorted into the grid-tier list at push
+        f[0] = log2f(1.f + (float)(adv0 ? fl0 : qn0 + ea));
         for (int b = 0; b < 8; ++b) f[1 + b] = (float)hb[b] * inv;
         f[9] = log2f(1.f + (float)buckets);
         f[10] = (float)reached_total / (float)I.n;
@@ -1849,6 +1962,8 @@ __device__ void solve_instance_async(const LaunchParams& P, const InstDesc& I, S
     C.local_rounds = 0;
     C.order_deg = I.order_degree;
     C.ring = true;
+    C.early = false;
+    C.want_hist = false;
     if (rank == 0 && threadIdx.x == 0) {
       // slots of the next bucket (their last user ended two barriers ago)
       const uint32_t sl = (p + 1) % 3;
@@ -1864,7 +1979,7 @@ __device__ void solve_instance_async(const LaunchParams& P, const InstDesc& I, S
       }
     }
     if (threadIdx.x < 8) sm.hist[threadIdx.x] = 0;
-    if (threadIdx.x < 3) sm.it_acc[threadIdx.x] = 0;
+    if (threadIdx.x < 4) sm.it_acc[threadIdx.x] = 0;
     if (threadIdx.x == 0) sm.phase_flag = 0;
     __syncthreads();
 
@@ -1877,6 +1992,8 @@ __device__ void solve_instance_async(const LaunchParams& P, const InstDesc& I, S
     S.ncnt = S.fcnt = S.scnt = 0;
     S.fmin = 0xffffffffu;
     S.credit = &sm.credit[warp];
+    S.hnext = sm.hist_next;
+    S.enext = &sm.it_acc[3];
     if (lane == 0) sm.credit[warp] = 0;
     uint32_t D = 0;        // ring units taken and processed, not yet subtracted from the pending total
     uint32_t sdone_w = 0;  // static items processed, not yet added to sdone

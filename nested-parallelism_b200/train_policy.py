@@ -149,7 +149,34 @@ def main():
     print("speedup (geomean) learned / plain:", report["speedup_geomean"], flush=True)
     if a.report:
         with open(a.report, "w") as f:
-            json.dump(report, f, indent=1)
+            json.dump(summary(report), f, indent=1)
+
+
+def summary(report):
+    """The committed record of a training run (policy_training.json): the plain
+    configuration, per-scale teacher gains, the winning schedules and the held-out
+    evaluation, from the full report `main` builds."""
+    by_scale = collections.defaultdict(list)
+    for r in report["teacher"]:
+        by_scale[r["scale"]].append(np.log(r["plain_ms"] / r["teacher_ms"]))
+    rnd = lambda r: {k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()}
+    return {
+        "what": "training and held-out evaluation of policy_weights.npz (nested-parallelism_b200/train_policy.py, "
+                "default arguments, one B200)",
+        "command": "python nested-parallelism_b200/train_policy.py --out nested-parallelism_b200/policy_weights.npz "
+                   "--report <file>",
+        "training_graphs": {"scales": report["scales"], "seeds_per_scale": report["seeds"],
+                            "full_search_seeds": report["search_seeds"], "topk": report["topk"]},
+        "plain_autotuned_on_scale20": report["plain"],
+        "records": report["records"],
+        "width_decisions": report["delta_decisions"],
+        "loss_first_last": [report["losses"][0], report["losses"][-1]],
+        "teacher_speedup_over_plain_by_scale": {str(k): float(np.exp(np.mean(v))) for k, v in sorted(by_scale.items())},
+        "schedule_wins_top10": dict(list(report["schedule_wins"].items())[:10]),
+        "eval_rmat22_seeds_1000_1009": [rnd(r) for r in report["eval"]],
+        "speedup_geomean_learned_over_plain": report["speedup_geomean"],
+        "wall_s": report["wall_s"],
+    }
 
 
 if __name__ == "__main__":
