@@ -58,7 +58,7 @@ extern "C" {
 #endif
 
 #define NPS_INF 0x40000000u  /* 1<<30, apps/sssp/src/gpu/sssp_wrapper.cu:7 */
-#define NPS_ABI_VERSION 2
+#define NPS_ABI_VERSION 3
 
 typedef int32_t nps_status;
 enum {
@@ -92,10 +92,11 @@ enum {
 /* The learned policy runs only on graphs of at least this many edges (unless
  * nps_params.policy_min_edges says otherwise); smaller ones run the plain kernel with
  * the same parameters (stats.policy_used says which).
- * Measured on held-out R-MAT graphs: below about 6 M edges (scale 18 at edge
- * factor 16) the policy's per-iteration cost outweighs what its bucket widths
- * save, above it the widths win (scale 19: 1.09x, 20: 1.23x, 22: 1.45x). */
-#define NPS_POLICY_MIN_EDGES 6000000
+ * Measured on held-out R-MAT graphs at edge factor 16 with the shipped weights: up
+ * to scale 16 (1 M edges) the policy's per-iteration cost outweighs what its bucket
+ * widths save (0.85-0.97x), at scale 17 it breaks even (1.02-1.05x), from scale 18
+ * (4 M edges) the widths win (18: 1.10-1.13x, 19: 1.18-1.22x, 22: 1.5x). */
+#define NPS_POLICY_MIN_EDGES 3000000
 
 typedef struct nps_params {
   int32_t level;            /* NPS_LEVEL_* (default NPS_LEVEL_BLOCK, the reference Makefile's CONSOLIDATE_LEVEL=1) */
@@ -130,7 +131,20 @@ typedef struct nps_params {
   int64_t policy_min_edges; /* NPS_POLICY_LEARNED runs only on graphs of at least this many edges,
                                smaller ones run the plain kernel; 0 (default) = NPS_POLICY_MIN_EDGES,
                                negative = no minimum */
+  int32_t sort_at_push;     /* iteration schedule: rows of at least the grid threshold that a warp pushes
+                               into the near queue join the grid-tier list when the warp flushes its
+                               pushes (walked the next iteration; otherwise they are sorted when taken
+                               from the queue and walked one iteration later).  1 = on, -1 = off,
+                               0 (default) = on when the grid threshold in effect is at most
+                               NPS_SORT_AT_PUSH_AUTO_MAX edges */
+  int32_t reserved2;        /* must be 0 */
 } nps_params;
+
+/* sort_at_push = 0 sorts at push time when the grid threshold is at most this: the flush
+ * reads row_ptr of every pushed vertex, which pays when many of them are grid-tier rows
+ * (R-MAT 22 at threshold 32: 23 -> 15 iterations) and costs when few are (a batch of
+ * scale 12-18 graphs at a hybrid grid threshold of 4096: 2.65 -> 2.98 ms). */
+#define NPS_SORT_AT_PUSH_AUTO_MAX 256
 
 /* How the persistent SSSP kernel moves from one frontier to the next. */
 enum {

@@ -224,6 +224,7 @@ class Params:
     bc_block_sources: int = 0           # bc: sources per block of dependency rows (0 = as memory allows)
     schedule: int = 0                   # SCHEDULE_ITERATIONS or SCHEDULE_ASYNC (see include/nps.h)
     policy_min_edges: int = 0           # learned policy only from this many edges (0: library default, <0: none)
+    sort_at_push: int = 0               # grid-tier rows sorted at push: 1 on, -1 off, 0 by the grid threshold
 
     def to_c(self, device_ptrs: bool, stream: Optional[int] = None) -> nps_params:
         p = nps_params()
@@ -243,6 +244,7 @@ class Params:
         p.reserved[1] = int(self.bc_block_sources)
         p.schedule = int(self.schedule)
         p.policy_min_edges = int(self.policy_min_edges)
+        p.sort_at_push = int(self.sort_at_push)
         return p
 
 

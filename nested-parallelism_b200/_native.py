@@ -36,7 +36,8 @@ class nps_params(C.Structure):
         ("device", C.c_int32), ("stream", C.c_void_p), ("timeout_s", C.c_double),
         ("trace", C.c_int32), ("light_heavy", C.c_int32), ("local_rounds", C.c_int32),
         ("order_degree", C.c_int32), ("delta_schedule", C.c_uint32), ("reserved", C.c_int32 * 2),
-        ("schedule", C.c_int32), ("policy_min_edges", C.c_int64),
+        ("schedule", C.c_int32), ("policy_min_edges", C.c_int64), ("sort_at_push", C.c_int32),
+        ("reserved2", C.c_int32),
     ]
 
 

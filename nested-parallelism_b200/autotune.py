@@ -38,9 +38,10 @@ AXES: Dict[str, List] = {
     "light_heavy": [False, True],
     "local_rounds": [0, 2, 8],
     "order_degree": [0, 32, 128],
+    "sort_at_push": [0, 1, -1],
 }
 ORDER = ["delta", "level", "threshold", "light_heavy", "order_degree", "grid_threshold", "block_size",
-         "local_rounds", "ctas_per_sm"]
+         "local_rounds", "ctas_per_sm", "sort_at_push"]
 
 
 @dataclasses.dataclass

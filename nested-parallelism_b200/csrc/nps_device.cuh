@@ -144,6 +144,7 @@ struct InstDesc {
   int32_t local_rounds; // warp-local processing rounds per vertex item (0 = none)
   int32_t order_degree; // rows below this degree ignore the bucket bound (0 = none)
   uint32_t dsched;      // per-bucket log2 widths, 4 bits each (0 = fixed delta)
+  int32_t sort_push;    // grid-tier rows sorted at push: 1 on, -1 off, 0 by the grid threshold
   int32_t async;        // 1: buckets are processed without per-iteration barriers (GRID tiers)
   unsigned long long* nq;  // near ring: slot = (tag << 32) | vertex, tag = index + 1 when filled
   uint32_t nq_mask;        // ring capacity - 1 (a power of two)
@@ -1577,7 +1578,8 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     C.ring = false;  // queues and lists of the iteration schedule
     level_thresholds(level, I.t1, I.t2, I.t3, C.t_warp, C.t_block, C.t_grid);
     // push-time sorting into the grid-tier list: plain iterations at the grid level
-    C.early = !heavy_it && C.sq == nullptr && C.t_grid != 0x7fffffff;
+    C.early = !heavy_it && C.sq == nullptr && C.t_grid != 0x7fffffff &&
+              (I.sort_push > 0 || (I.sort_push == 0 && C.t_grid <= NPS_SORT_AT_PUSH_AUTO_MAX));
     C.want_hist = want_iter;
     const int4* Hprev = I.heavy + ((it & 1) ? 0 : hhalf);
     const int32_t* Hitem = I.hitem + ((it & 1) ? 0 : I.icap);

@@ -408,6 +408,8 @@ nps_status check_params(const nps_params& p) {
   if (p.delta >= NPS_INF) return nps_fail(NPS_ERR_INVALID_ARG, "delta must be < 2^30");
   if (p.local_rounds < 0 || p.local_rounds > 1024) return nps_fail(NPS_ERR_INVALID_ARG, "local_rounds must be in [0, 1024]");
   if (p.order_degree < 0) return nps_fail(NPS_ERR_INVALID_ARG, "order_degree must be >= 0");
+  if (p.sort_at_push < -1 || p.sort_at_push > 1) return nps_fail(NPS_ERR_INVALID_ARG, "sort_at_push must be -1, 0 or 1");
+  if (p.reserved2 != 0) return nps_fail(NPS_ERR_INVALID_ARG, "reserved2 must be 0");
   return NPS_OK;
 }
 
@@ -456,6 +458,7 @@ void fill_thresholds(const nps_params& p, InstDesc& d) {
   d.local_rounds = p.local_rounds;
   d.order_degree = p.order_degree;
   d.dsched = p.delta_schedule;
+  d.sort_push = p.sort_at_push;
 }
 
 // Whether a single-instance call runs the asynchronous schedule: requested, tiers

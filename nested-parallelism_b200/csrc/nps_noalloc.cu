@@ -224,6 +224,7 @@ extern "C" nps_status nps_sssp_noalloc(const int32_t* d_row_ptr, const int32_t* 
   d.local_rounds = p.local_rounds < 0 ? 0 : (p.local_rounds > 1024 ? 1024 : p.local_rounds);
   d.order_degree = p.order_degree < 0 ? 0 : p.order_degree;
   d.dsched = p.delta_schedule;
+  d.sort_push = p.sort_at_push < -1 ? -1 : (p.sort_at_push > 1 ? 1 : p.sort_at_push);
 
   const TeamDesc td{0, grid, 0, 1};
   LaunchParams lp;

@@ -39,7 +39,7 @@ def test_header_compiles_as_c_and_links(tmp_path):
     subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", f"-I{os.path.join(ROOT, 'include')}", str(src), "-o",
                     str(exe), f"-L{LIBDIR}", "-lnps", f"-Wl,-rpath,{LIBDIR}"], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
-    assert out == ["2", "1", "64", str(0x40000000)]  # ABI 2: nps_params grew policy_min_edges
+    assert out == ["3", "1", "64", str(0x40000000)]  # ABI 3: nps_params grew sort_at_push
 
 
 def test_params_defaults_match_the_reference_build(nps):

@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 
 WEIGHTS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
                        "nested-parallelism_b200", "policy_weights.npz")
-MIN_EDGES = 6_000_000  # NPS_POLICY_MIN_EDGES in include/nps.h
+MIN_EDGES = 3_000_000  # NPS_POLICY_MIN_EDGES in include/nps.h
 
 
 def _median_ms(nps, dg, p, reps=9):
