@@ -1443,6 +1443,14 @@ __device__ bool start_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     for (uint32_t v = gtid; v < (uint32_t)I.n; v += gthreads) {
       I.dist[v] = (v == (uint32_t)I.src) ? 0u : kInf;
       if (wrap) { I.mark[v] = 0; I.fmark[v] = 0; I.smark[v] = 0; }
+      if ((v & 7u) == 0) {
+        // the stamps and row offsets are read at random for the whole run: bring them into
+        // L2 with the evict-last priority while the distances are written (R-MAT 22: DRAM
+        // bytes 1.383 -> 1.359 GB, 1 % faster)
+        asm volatile("prefetch.global.L2::evict_last [%0];" ::"l"(I.mark + v));
+        asm volatile("prefetch.global.L2::evict_last [%0];" ::"l"(I.fmark + v));
+        asm volatile("prefetch.global.L2::evict_last [%0];" ::"l"(I.row_ptr + v));
+      }
     }
     if (rank == 0 && threadIdx.x == 0) {
       I.q[0][0] = I.src;
