@@ -1382,7 +1382,9 @@ def main():
     ap.add_argument("--workload", default="rmat22", choices=sorted(WORKLOADS))
     ap.add_argument("--delta", type=int, default=None)
     ap.add_argument("--level", type=int, default=None)
-    ap.add_argument("--policy", default="learned", choices=["plain", "learned"])
+    ap.add_argument("--policy", default=None, choices=["plain", "learned"],
+                    help="arm reported as `value` (default: learned for rmat22, the learned-policy workload, "
+                         "plain for the plain-SSSP workloads rmat20, grid4096 and uniform16k)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--tune-budget", type=int, default=24, help="autotuner evaluations before timing")
@@ -1391,6 +1393,8 @@ def main():
                     help="SSSP schedule of both arms: frontier iterations with a team barrier each, or asynchronous "
                          "buckets (NPS_SCHEDULE_ASYNC)")
     a = ap.parse_args()
+    if a.policy is None:
+        a.policy = "learned" if a.workload == "rmat22" else "plain"
     a.warmup = max(a.warmup, 3)
     a.seeds = tuple(int(x) for x in a.seeds.split(",")) if a.seeds else None
 

@@ -95,7 +95,12 @@ struct __align__(128) Counters {
   uint32_t pend;
   uint32_t swork[3];
   uint32_t sdone[3];
-  uint32_t pad2[5];
+  // settle-list entries appended in each iteration, slot = iteration % 3.  The decision
+  // after an iteration reads its own slot, which the next iteration leaves alone (that
+  // iteration may already be appending while a slower CTA decides: a bucket advance
+  // appends the far-pile vertices it processes)
+  uint32_t sadd[3];
+  uint32_t pad2[2];
   // striped work counters, one 128-byte line each: work[slot][stripe * 32]
   uint32_t work[3][kStripes * 32];
 };
@@ -376,6 +381,7 @@ struct IterCtx {
   int32_t order_deg;     // improved vertices below this degree join the near queue at any distance
   bool ring;             // asynchronous bucket: near pushes go to the near ring, grid-tier rows
                          // to the segment ring (qn, heavy and the item tables are unused)
+  uint32_t* sadd;        // counts this iteration's settle-list appends
   bool early;            // near pushes of at least t_grid edges join this iteration's grid-tier
                          // list when their staging buffer is flushed (walked next iteration)
   bool want_hist;        // policy features or trace: count the degrees of those rows
@@ -588,10 +594,14 @@ struct Stage {
 
 // Move the first `nflush` staged entries to q and shift the rest down.
 __device__ __forceinline__ void stage_flush(int32_t* buf, uint32_t& cnt, uint32_t nflush, int32_t* q,
-                                            uint32_t* tail, uint32_t cap, uint32_t* status, int lane) {
+                                            uint32_t* tail, uint32_t cap, uint32_t* status, int lane,
+                                            uint32_t* count = nullptr) {
   __syncwarp();
   uint32_t base = 0;
-  if (lane == 0) base = atomicAdd(tail, nflush);
+  if (lane == 0) {
+    base = atomicAdd(tail, nflush);
+    if (count) atomicAdd(count, nflush);
+  }
   base = __shfl_sync(kFull, base, 0);
   for (uint32_t i = lane; i < nflush; i += 32) {
     if (base + i < cap) q[base + i] = buf[i];
@@ -672,7 +682,8 @@ __device__ __forceinline__ void ring_flush(const InstDesc& I, int32_t* buf, uint
 template <int K>
 __device__ __forceinline__ void stage_k(int32_t* buf, uint32_t& cnt, const bool (&f)[K], const int32_t (&v)[K],
                                         int32_t* q, uint32_t* tail, uint32_t cap, uint32_t* status, int lane,
-                                        const InstDesc* ring = nullptr, uint32_t* credit = nullptr) {
+                                        const InstDesc* ring = nullptr, uint32_t* credit = nullptr,
+                                        uint32_t* count = nullptr) {
   uint32_t b[K];
   uint32_t tot = 0;
 #pragma unroll
@@ -691,7 +702,7 @@ __device__ __forceinline__ void stage_k(int32_t* buf, uint32_t& cnt, const bool 
   cnt += tot;
   if (cnt >= (uint32_t)kFlushAt) {
     if (ring) ring_flush(*ring, buf, cnt, cnt & ~31u, lane, credit);
-    else stage_flush(buf, cnt, cnt & ~31u, q, tail, cap, status, lane);
+    else stage_flush(buf, cnt, cnt & ~31u, q, tail, cap, status, lane, count);
   }
 }
 
@@ -790,7 +801,7 @@ __device__ __forceinline__ void stage_drain(const InstDesc& I, Stage& S, const I
     else stage_flush(S.nbuf, S.ncnt, S.ncnt, C.qn, C.qn_tail, qcap, status, lane);
   }
   if (S.fcnt) stage_flush(S.fbuf, S.fcnt, S.fcnt, C.fp, C.fp_tail, qcap, status, lane);
-  if (S.scnt) stage_flush(S.sbuf, S.scnt, S.scnt, C.sq, C.sq_tail, qcap, status, lane);
+  if (S.scnt) stage_flush(S.sbuf, S.scnt, S.scnt, C.sq, C.sq_tail, qcap, status, lane, C.sadd);
 }
 
 template <int K>
@@ -1161,7 +1172,7 @@ __device__ __forceinline__ void process_vertex_item(const InstDesc& I, const Ite
     bool f[1] = {false};
     if (deg > 0 && __ldcg(I.smark + v) != C.sstamp) f[0] = atomicExch(I.smark + v, C.sstamp) != C.sstamp;
     const int32_t vv[1] = {v};
-    stage_k<1>(S.sbuf, S.scnt, f, vv, C.sq, C.sq_tail, I.qcap, &I.ctr->status, lane);
+    stage_k<1>(S.sbuf, S.scnt, f, vv, C.sq, C.sq_tail, I.qcap, &I.ctr->status, lane, nullptr, nullptr, C.sadd);
   }
   // deferred entries remember which edges they relax in the top bit of the vertex id
   // deferred entries remember which edges they relax in the top bit of the vertex id
@@ -1548,6 +1559,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
   bool heavy_it = false;  // this iteration relaxes the heavy edges of the settle list
   uint32_t hg = 0;        // settle-list generation
   uint32_t slen = 0;
+  uint32_t s_gen = 0;     // entries appended to the settle list of generation hg so far
   uint32_t adv_len = 0, T_old = 0;
   uint32_t hprev_cnt = 0;
   unsigned long long hprev_tot = 0;
@@ -1581,6 +1593,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     C.sq = (C.split != 0u && !heavy_it) ? I.sq[hg & 1] : nullptr;
     C.sq_tail = &ctr->stail[hg % 3];
     C.sstamp = base + hg + 1;
+    C.sadd = &ctr->sadd[it % 3];
     C.local_rounds = heavy_it ? 0 : I.local_rounds;  // a heavy pass only relaxes heavy edges
     C.order_deg = I.order_degree;
     C.ring = false;  // queues and lists of the iteration schedule
@@ -1599,6 +1612,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
         ctr->heavy[(it + 1) % 3] = 0;
         ctr->ftail[(E + 1) % 3] = 0;
         ctr->fmin[(E + 1) % 3] = 0xffffffffu;
+        ctr->sadd[(it + 1) % 3] = 0;
         if (heavy_it) ctr->stail[(hg + 1) % 3] = 0;
         if (want_iter) {
           const uint32_t sl = (it + 1) % 3;
@@ -1768,7 +1782,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
       const unsigned long long h1 = ld_relaxed_u64(&ctr->heavy[it % 3]);
       const uint32_t f1 = __ldcg(&ctr->ftail[ep % 3]);
       const uint32_t m1 = __ldcg(&ctr->fmin[ep % 3]);
-      const uint32_t s1 = __ldcg(&ctr->stail[hg % 3]);
+      const uint32_t s1 = __ldcg(&ctr->sadd[it % 3]);
       const uint32_t st1 = ld_relaxed_u32(&ctr->status);
       uint32_t hb[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       unsigned long long ie = 0, ii = 0;
@@ -1797,7 +1811,10 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
         const uint32_t qn0 = min(q1, I.qcap);
         const uint32_t fl0 = min(f1, I.qcap);
         const uint32_t hn0 = min((uint32_t)(h1 >> kHeavyShift), hhalf);
-        const bool adv0 = qn0 == 0 && hn0 == 0 && fl0 != 0;
+        // an advance follows only when no heavy pass does (the far-pile length is stable only
+        // then: a light or heavy pass may already be pushing to it in a faster CTA)
+        const bool heavy0 = I.light_heavy && delta != 0 && min(s_gen + s1, I.qcap) != 0;
+        const bool adv0 = qn0 == 0 && hn0 == 0 && !heavy0 && fl0 != 0;
         float hs = 0.f;
         for (int b = 0; b < 8; ++b) hs += (float)hb[b];
         const float inv = hs > 0.f ? 1.f / hs : 0.f;
@@ -1843,13 +1860,16 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     hprev_cnt = hn;
     hprev_tot = hc & kHeavyMask;
     advance = false;
-    const uint32_t sn = min(sm.bc_s, I.qcap);
+    // entries of the current settle list: every CTA adds the same per-iteration counts
+    s_gen += sm.bc_s;
+    const uint32_t sn = min(s_gen, I.qcap);
     const bool split_now = I.light_heavy && delta != 0;
     heavy_it = false;
     if (qn == 0 && hn == 0 && split_now && sn != 0) {
       // bucket drained: relax the heavy edges of every vertex it settled, once
       heavy_it = true;
       slen = sn;
+      s_gen = 0;  // the heavy iteration appends nothing; the next list starts empty
     } else if (qn == 0 && hn == 0) {
       if (fl == 0) {
         it += 1;
@@ -1972,6 +1992,7 @@ __device__ void solve_instance_async(const LaunchParams& P, const InstDesc& I, S
     C.local_rounds = 0;
     C.order_deg = I.order_degree;
     C.ring = true;
+    C.sadd = nullptr;
     C.early = false;
     C.want_hist = false;
     if (rank == 0 && threadIdx.x == 0) {
