@@ -245,7 +245,13 @@ nps_status nps_write_dimacs9(const char* path, const nps_graph* g, int32_t sourc
 /* ---- SSSP --------------------------------------------------------------- */
 /* Single source.  row_ptr[n+1], col[m], w[m]; dist_out[n] receives distances
  * (NPS_INF = unreachable).  Pointers are host or device per p->device_ptrs.
- * Uses a per-device default context.  p may be NULL (defaults). */
+ * Uses a per-device default context.  p may be NULL (defaults).
+ * Host pointers: the CSR is copied to a cached device workspace on every call and
+ * the distances copied back (pinned host buffers copy fastest).  On graphs of at
+ * least 2^20 edges whose largest weight fits in 8 or 16 bits, the weights cross
+ * PCIe packed (one host pass with OpenMP threads, overlapped with the column copy)
+ * and are widened on the device; the context keeps a pinned staging buffer of
+ * 2 bytes per edge for this. */
 nps_status nps_sssp(const int32_t* row_ptr, const int32_t* col, const uint32_t* w, int32_t n,
                     int64_t m, int32_t src, const nps_params* p, uint32_t* dist_out,
                     nps_stats* st);
