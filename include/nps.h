@@ -70,7 +70,8 @@ enum {
   NPS_ERR_NO_DEVICE = 5,     /* no CUDA device / wrong architecture */
   NPS_ERR_IO = 6,            /* file could not be opened or parsed */
   NPS_ERR_FORMAT = 7,        /* malformed CSR or input file */
-  NPS_ERR_OOM = 8            /* host or device allocation failed */
+  NPS_ERR_OOM = 8,           /* host or device allocation failed */
+  NPS_ERR_INTERNAL = 9       /* the CTAs of a persistent kernel took different schedule decisions */
 };
 
 /* Consolidation granularity for vertices whose out-degree is at least
@@ -125,6 +126,9 @@ typedef struct nps_params {
   int32_t reserved[2];      /* reserved[0] = 1: test hook, the first in-kernel barrier (of the SSSP
                                kernel, or of nps_color's round kernel) waits for an arrival that
                                never comes, so its bounded wait must expire.
+                               reserved[0] = 2: test hook, CTA 1 of the SSSP kernel reports another
+                               hash for its first schedule decision, so the agreement check must
+                               end the run with NPS_ERR_INTERNAL.
                                reserved[1] > 0: nps_bc folds at most this many sources per block
                                of dependency rows (0 = as many as 2 GB of rows hold) */
   int32_t schedule;         /* NPS_SCHEDULE_* (default NPS_SCHEDULE_ITERATIONS) */

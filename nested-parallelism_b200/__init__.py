@@ -221,6 +221,7 @@ class Params:
     order_degree: int = 0               # delta > 0: rows below this degree ignore the bucket bound
     delta_schedule: int = 0             # per-bucket log2 widths, 4 bits each (see delta_schedule())
     fault_inject_wait: bool = False     # test hook: the first barrier can never complete
+    fault_inject_disagree: bool = False  # test hook: CTA 1 reports another decision hash (NPS_ERR_INTERNAL)
     bc_block_sources: int = 0           # bc: sources per block of dependency rows (0 = as memory allows)
     schedule: int = 0                   # SCHEDULE_ITERATIONS or SCHEDULE_ASYNC (see include/nps.h)
     policy_min_edges: int = 0           # learned policy only from this many edges (0: library default, <0: none)
@@ -240,7 +241,7 @@ class Params:
         p.delta_schedule = int(self.delta_schedule) & 0xFFFFFFFF
         p.device_ptrs = int(bool(device_ptrs))
         p.stream = stream
-        p.reserved[0] = int(bool(self.fault_inject_wait))
+        p.reserved[0] = 2 if self.fault_inject_disagree else int(bool(self.fault_inject_wait))
         p.reserved[1] = int(self.bc_block_sources)
         p.schedule = int(self.schedule)
         p.policy_min_edges = int(self.policy_min_edges)

@@ -24,7 +24,7 @@ NPS_MLP_IN, NPS_MLP_HID, NPS_MLP_OUT = 12, 32, 14
 STATUS_NAMES = {
     0: "NPS_OK", 1: "NPS_ERR_INVALID_ARG", 2: "NPS_ERR_CUDA", 3: "NPS_ERR_CAPACITY",
     4: "NPS_ERR_TIMEOUT", 5: "NPS_ERR_NO_DEVICE", 6: "NPS_ERR_IO", 7: "NPS_ERR_FORMAT",
-    8: "NPS_ERR_OOM",
+    8: "NPS_ERR_OOM", 9: "NPS_ERR_INTERNAL",
 }
 
 

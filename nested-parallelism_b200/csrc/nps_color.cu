@@ -591,7 +591,7 @@ extern "C" nps_status nps_color(const int32_t* row_ptr, const int32_t* col, int3
     uint32_t* bar = W->bar;
     uint32_t* abort_word = W->bar + 1;
     unsigned long long timeout_ns = (unsigned long long)(p.timeout_s * 1e9);
-    uint32_t inject = p.reserved[0] != 0 ? 1u : 0u;  // test hook: the first barrier cannot complete
+    uint32_t inject = p.reserved[0] == 1 ? 1u : 0u;  // test hook: the first barrier cannot complete
     void* args[] = {&a, &bar, &abort_word, &timeout_ns, &inject};
     NPS_CUDA_RETURN(cudaLaunchCooperativeKernel((const void*)color_rounds_kernel, dim3(rgrid), dim3(kThreads), args, 0, s));
   }

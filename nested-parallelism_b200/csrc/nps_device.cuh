@@ -102,7 +102,10 @@ struct __align__(128) Counters {
   uint32_t sadd[3];
   uint32_t pad2[2];
   // striped work counters, one 128-byte line each: work[slot][stripe * 32]
-  uint32_t work[3][kStripes * 32];
+  // decision agreement: every CTA adds a hash of the counters its decision after iteration
+  // i read to slot i % 4, and checks the sum one iteration later (team size x its own hash)
+  uint32_t agree[4];
+  alignas(128) uint32_t work[3][kStripes * 32];
 };
 
 // Work rings of the asynchronous buckets.  Head and tail counters persist across
@@ -182,6 +185,7 @@ struct LaunchParams {
   const TeamDesc* teams;
   int32_t n_teams;
   int32_t fault_inject_wait;  // 1: the first barrier waits for an arrival that never comes
+  int32_t test_disagree;      // 1: CTA 1 reports another hash for the first decision (agreement check test)
   uint32_t* bar;              // per-team barrier words (see team_barrier), bar_stride words per team
   uint32_t bar_stride;
   uint32_t* abort_flag;
@@ -888,6 +892,8 @@ struct Smem {
   uint32_t bc_q, bc_f, bc_m, bc_s;   // counters broadcast after a barrier
   unsigned long long bc_h;
   unsigned long long t_start;
+  uint32_t agree_prev;         // thread 0: hash of this CTA's last schedule decision
+  uint32_t bc_ag;              // the agreement slot of the decision before it
 };
 
 // Team barrier over the CTAs of one team.  Bounded: gives up after timeout_ns
@@ -1435,6 +1441,29 @@ __device__ __forceinline__ void level_thresholds(int level, int32_t thr, int32_t
   }
 }
 
+// Decision agreement (thread 0 of each CTA).  After a barrier every CTA reads the
+// counters its next decision depends on; they must be identical in every CTA (the
+// decision also depends on per-CTA state, which stays identical as long as every earlier
+// decision was).  Each CTA adds a hash of what it read to slot it % 4 and checks, one
+// iteration later, that the slot of the previous decision holds team_size times its own
+// hash (prev_sum: that slot, loaded by the caller with its other counters).  False on a
+// mismatch.  Out of line, so the hot loop's register allocation does not pay for it.
+static __device__ __noinline__ bool agree_step(Counters* ctr, uint32_t it, uint32_t team_size, uint32_t* prev,
+                                               uint32_t prev_sum, uint32_t a, uint32_t b, uint32_t c, uint32_t d,
+                                               uint32_t e, uint32_t f) {
+  const bool ok = it == 0 || prev_sum == *prev * team_size;
+  uint32_t h = 0x811C9DC5u;  // FNV-1a over the words
+  h = (h ^ a) * 0x01000193u;
+  h = (h ^ b) * 0x01000193u;
+  h = (h ^ c) * 0x01000193u;
+  h = (h ^ d) * 0x01000193u;
+  h = (h ^ e) * 0x01000193u;
+  h = (h ^ f) * 0x01000193u;
+  atomicAdd(&ctr->agree[it % 4], h);
+  *prev = h;
+  return ok;
+}
+
 // Start of a solve, shared by both schedules: distances and stamps, the initial
 // frontier in q[0] (the source, or the state form's flagged vertices), a team
 // barrier, then the first bucket's width and level (from the policy's start state
@@ -1613,6 +1642,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
         ctr->ftail[(E + 1) % 3] = 0;
         ctr->fmin[(E + 1) % 3] = 0xffffffffu;
         ctr->sadd[(it + 1) % 3] = 0;
+        ctr->agree[(it + 1) % 4] = 0;  // last read by the decision after iteration it - 2
         if (heavy_it) ctr->stail[(hg + 1) % 3] = 0;
         if (want_iter) {
           const uint32_t sl = (it + 1) % 3;
@@ -1631,6 +1661,16 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     }
     if (threadIdx.x < 4) sm.it_acc[threadIdx.x] = 0;
     __syncthreads();
+    if (threadIdx.x == 0 && it > 0 &&
+        !agree_step(ctr, it - 1, team_size, &sm.agree_prev, sm.bc_ag,
+                    sm.bc_q + ((P.test_disagree && rank == 1 && it == 1) ? 1u : 0u), (uint32_t)sm.bc_h,
+                    (uint32_t)(sm.bc_h >> 32), sm.bc_m, sm.bc_s, advance ? sm.bc_f : 0u)) {
+      // the decision that opened this iteration was not the same in every CTA.  It is
+      // checked here, off the decision's path, while the other warps start working; the
+      // far-pile tail counts only after an advance, the one decision after which it is stable
+      atomicCAS(&ctr->status, 0u, (uint32_t)NPS_ERR_INTERNAL);
+      atomicExch(P.abort_flag, 1u);
+    }
 
     const int32_t* srcq = advance ? I.fq[ep & 1] : (heavy_it ? I.sq[hg & 1] : I.q[it & 1]);
     const uint32_t srclen = advance ? adv_len : (heavy_it ? slen : qlen);
@@ -1779,6 +1819,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     if (threadIdx.x == 0) {
       const uint32_t sl = it % 3;
       const uint32_t q1 = __ldcg(&ctr->qtail[(it + 1) % 3]);
+      const uint32_t ag = __ldcg(&ctr->agree[(it + 3) % 4]);
       const unsigned long long h1 = ld_relaxed_u64(&ctr->heavy[it % 3]);
       const uint32_t f1 = __ldcg(&ctr->ftail[ep % 3]);
       const uint32_t m1 = __ldcg(&ctr->fmin[ep % 3]);
@@ -1799,6 +1840,7 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
       sm.bc_f = f1;
       sm.bc_m = m1;
       sm.bc_s = s1;
+      sm.bc_ag = ag;
       if (st1 != 0) {
         atomicExch(P.abort_flag, 1u);
         sm.ok = 0;

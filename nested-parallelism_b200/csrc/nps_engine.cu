@@ -532,6 +532,8 @@ nps_status status_from_device(uint32_t st) {
     case NPS_ERR_CAPACITY: return nps_fail(NPS_ERR_CAPACITY, "device queue capacity exceeded");
     case NPS_ERR_TIMEOUT: return nps_fail(NPS_ERR_TIMEOUT, "a bounded wait in the persistent kernel timed out");
     case NPS_ERR_FORMAT: return nps_fail(NPS_ERR_FORMAT, "malformed CSR: a row range or neighbour id is out of bounds");
+    case NPS_ERR_INTERNAL:
+      return nps_fail(NPS_ERR_INTERNAL, "the persistent kernel's CTAs took different schedule decisions");
     default: return nps_fail((nps_status)st, "device reported error " + std::to_string(st));
   }
 }
@@ -635,7 +637,8 @@ nps_status run_single(nps_ctx* c, cudaStream_t s, const int32_t* row, const int3
   lp.inst = nullptr;
   lp.order = nullptr;
   lp.n_teams = 1;
-  lp.fault_inject_wait = p.reserved[0] != 0;
+  lp.fault_inject_wait = p.reserved[0] == 1;
+  lp.test_disagree = p.reserved[0] == 2;
   lp.bar = ctl.bar();
   lp.bar_stride = (uint32_t)ctl.stride;
   lp.abort_flag = ctl.abort_flag();
@@ -1117,7 +1120,8 @@ extern "C" nps_status nps_sssp_batch(const nps_instance* inst, int32_t count, co
   lp.order = c->b_order.p;
   lp.teams = c->b_teams.p;
   lp.n_teams = c->b_nteams;
-  lp.fault_inject_wait = p.reserved[0] != 0;
+  lp.fault_inject_wait = p.reserved[0] == 1;
+  lp.test_disagree = p.reserved[0] == 2;
   lp.bar = ctl.bar();
   lp.bar_stride = (uint32_t)ctl.stride;
   lp.abort_flag = ctl.abort_flag();

@@ -231,7 +231,8 @@ extern "C" nps_status nps_sssp_noalloc(const int32_t* d_row_ptr, const int32_t* 
   memset(&lp, 0, sizeof(lp));
   lp.teams = (const TeamDesc*)(base + kOffTeam);
   lp.n_teams = 1;
-  lp.fault_inject_wait = p.reserved[0] != 0;
+  lp.fault_inject_wait = p.reserved[0] == 1;
+  lp.test_disagree = p.reserved[0] == 2;
   lp.bar = (uint32_t*)(base + kOffBar);
   lp.bar_stride = (uint32_t)stride;
   lp.abort_flag = (uint32_t*)(base + kOffAbort);

@@ -31,3 +31,17 @@ def test_light_heavy_bucket_advances_stay_exact_over_many_runs(nps, oracle, cuda
         d = dg.dist.cpu().numpy().view(np.uint32)
         bad = int((d != want).sum())
         assert st.status == 0 and bad == 0, f"run {r}: {bad} mismatches, {st.iterations} iterations, {st.buckets} buckets"
+
+
+def test_a_disagreement_is_reported_and_the_context_survives(nps, oracle, cuda_device):
+    """The agreement check itself: with the test hook, CTA 1 adds another hash for the
+    first decision (it still takes the same one), so every CTA finds the sum wrong one
+    iteration later and the run ends with NPS_ERR_INTERNAL instead of a result.  No GPU
+    fault is involved; the next call must be exact."""
+    g = nps.gen_uniform(16384, 131072, 100, 1)
+    with pytest.raises(nps.NpsError) as e:
+        nps.sssp(g, 0, nps.Params(level=2, fault_inject_disagree=True))
+    assert e.value.status == 9  # NPS_ERR_INTERNAL
+    dist, st = nps.sssp(g, 0, nps.Params(level=2))
+    assert st.status == 0
+    assert np.array_equal(dist, oracle.sssp_heap(g.row_ptr, g.col, g.w, 0))
