@@ -286,12 +286,14 @@ nps_status nps_trace_read(int32_t device, nps_trace_rec* out, int32_t cap, int32
  * static __device__ array of NPS_NOALLOC_SCRATCH_BYTES (10 MiB) that every GPU
  * loading libnps holds until exit.
  * Limit: n <= NPS_NOALLOC_MAX_VERTICES (larger graphs get NPS_ERR_CAPACITY).
- * The call synchronises its stream to return a status, so it cannot run on a
- * stream being captured into a CUDA graph (NPS_ERR_INVALID_ARG there).  The
- * first call on a device resolves the array's address and caches it (again after
- * a cudaDeviceReset() of that device).  Calls share
- * the array: calls whose kernels overlap on the GPU race, so order them on one
- * stream.  No trace, no kernel_ms in the stats.
+ * The call synchronises its stream to return a status; on a stream that is being
+ * captured it returns NPS_ERR_INVALID_ARG.  The first call on a device resolves
+ * the array's device address (cudaGetSymbolAddress, that device current) and
+ * caches it (again after a cudaDeviceReset() of that device): make that first call
+ * before any stream capture begins.  Calls share the array and it keeps the last
+ * call's contents (what must start at zero is cleared on every call): calls whose
+ * kernels overlap on the GPU race, so order them on one stream.  No trace, no
+ * kernel_ms in the stats.
  * Device pointers only; p->stream selects the stream (NULL = legacy default). */
 #define NPS_NOALLOC_MAX_VERTICES 131072
 #define NPS_NOALLOC_SCRATCH_BYTES (10u << 20)

@@ -9,9 +9,8 @@
 // graph arrives; this one never calls cudaMalloc, cudaFree, cudaMallocHost,
 // stream or event creation.
 //
-// Not for stream capture.  The call waits for its kernel (it copies the run's
-// counters to the host and synchronises the stream to return a status), which a
-// stream being captured into a CUDA graph does not allow; on a capturing stream
+// The call waits for its kernel: it copies the run's counters to the host and
+// synchronises the stream to return a status.  On a stream that is being captured
 // it returns NPS_ERR_INVALID_ARG before doing anything.
 //
 // How.  The workspace the persistent kernel needs (queues, dedupe stamps, the
@@ -21,9 +20,9 @@
 // Every GPU that loads libnps holds this array until the process exits.  The
 // array's host-side name is only a stand-in for the symbol, not a device
 // address, so the first call on each device resolves the address with
-// cudaGetSymbolAddress (that device current) and caches it; after a
-// cudaDeviceReset() of that device the module is loaded anew, so the address is
-// resolved again on the next call.
+// cudaGetSymbolAddress (that device current) and caches it; make that first call
+// before any stream capture begins.  After a cudaDeviceReset() of that device the
+// module is loaded anew, so the address is resolved again on the next call.
 //
 // Sharing.  All calls on a device share the one array and it keeps the state of
 // the last call: counters and barrier words are cleared at the start of each

@@ -7,8 +7,8 @@ serves them from a static device array sized for graphs of up to
 NPS_NOALLOC_MAX_VERTICES vertices.  Its distances must equal the CPU oracle's
 Dijkstra and the regular entry point's bit for bit (integer distances: zero
 tolerance), and must stay equal on a second call in a row, since calls reuse
-the same array.  The call synchronises its stream, so it refuses a stream that
-is being captured into a CUDA graph.
+the same array.  The call synchronises its stream to return a status; on a
+stream that is being captured it returns NPS_ERR_INVALID_ARG.
 
 This file is named to be collected last, so a run that stops at the first
 failure has already run every other test.
