@@ -140,7 +140,9 @@ typedef struct nps_params {
                                pushes (walked the next iteration; otherwise they are sorted when taken
                                from the queue and walked one iteration later).  1 = on, -1 = off,
                                0 (default) = on when the grid threshold in effect is at most
-                               NPS_SORT_AT_PUSH_AUTO_MAX edges */
+                               NPS_SORT_AT_PUSH_AUTO_MAX edges and the edges have weights (off for
+                               nps_bfs, where every reached row is walked once anyway: R-MAT 22
+                               BFS takes 0.645 ms with it off, 0.682 ms with it on) */
   int32_t reserved2;        /* must be 0 */
 } nps_params;
 

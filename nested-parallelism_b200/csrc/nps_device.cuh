@@ -1629,7 +1629,8 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
     level_thresholds(level, I.t1, I.t2, I.t3, C.t_warp, C.t_block, C.t_grid);
     // push-time sorting into the grid-tier list: plain iterations at the grid level
     C.early = !heavy_it && C.sq == nullptr && C.t_grid != 0x7fffffff &&
-              (I.sort_push > 0 || (I.sort_push == 0 && C.t_grid <= NPS_SORT_AT_PUSH_AUTO_MAX));
+              (I.sort_push > 0 ||
+               (I.sort_push == 0 && C.t_grid <= NPS_SORT_AT_PUSH_AUTO_MAX && I.w != nullptr));
     C.want_hist = want_iter;
     const int4* Hprev = I.heavy + ((it & 1) ? 0 : hhalf);
     const int32_t* Hitem = I.hitem + ((it & 1) ? 0 : I.icap);
