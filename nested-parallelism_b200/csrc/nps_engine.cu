@@ -767,7 +767,12 @@ nps_status ensure_pinned_wpack(nps_ctx* c, size_t bytes) {
   if (c->h_wpack) cudaFreeHost(c->h_wpack);
   c->h_wpack = nullptr;
   c->h_wpack_n = 0;
-  NPS_CUDA(cudaMallocHost(&c->h_wpack, bytes));
+  const cudaError_t err = cudaMallocHost(&c->h_wpack, bytes);
+  if (err != cudaSuccess) {
+    cudaGetLastError();
+    c->h_wpack = nullptr;
+    return nps_fail(NPS_ERR_OOM, std::string("pinned weight staging: cudaMallocHost: ") + cudaGetErrorString(err));
+  }
   c->h_wpack_n = bytes;
   return NPS_OK;
 }
@@ -810,8 +815,13 @@ nps_status sssp_ctx_impl(nps_ctx* c, const int32_t* row_ptr, const int32_t* col,
       if (!bfs) {
         int wb = 4;
         if (m >= kPackMinEdges) {
-          if ((e = ensure_pinned_wpack(c, 2 * (size_t)m))) return e;
-          wb = pack_weights(w, m, c->h_wpack);  // overlaps the copies queued above
+          if (ensure_pinned_wpack(c, 2 * (size_t)m) == NPS_OK) {
+            wb = pack_weights(w, m, c->h_wpack);  // overlaps the copies queued above
+          } else {
+            // no pinned staging of that size: copy the weights as they are
+            cudaGetLastError();
+            nps_clear_error();
+          }
         }
         if (wb == 4) {
           NPS_CUDA(cudaMemcpyAsync(c->g_w.p, w, sizeof(uint32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
