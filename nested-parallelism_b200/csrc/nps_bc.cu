@@ -50,7 +50,6 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int32_t kMaxLevel = 9999;
 constexpr int32_t kWarpRow = 32;  // rows of at least this many edges are walked by a warp (forward)
-constexpr unsigned kFull = 0xffffffffu;
 
 struct BcArgs {
   const int32_t* row;

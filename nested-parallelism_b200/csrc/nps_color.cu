@@ -213,26 +213,11 @@ __global__ void color_first_kernel(ColorArgs a) {
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(&a.c->max_color, 1);  // vertex 0 is always ready
 }
 
-// One dependant w of a vertex of color cv: best[w] rises to cv, a fence orders
-// that before the decrement of pending[w], and the decrement that takes it to
-// 0 (after a second fence) reads best and colors w with best + 1.  Returns the
-// color given (0 when w is still waiting).
-__device__ __forceinline__ int32_t settle(const ColorArgs& a, int32_t w, int32_t cv, int32_t* out, uint32_t* len) {
-  atomicMax(a.best + w, cv);
-  __threadfence();
-  if (atomicSub(a.pending + w, 1) != 1) return 0;
-  __threadfence();
-  const int32_t cw = __ldcg(a.best + w) + 1;
-  a.color[w] = cw;
-  out[atomicAdd(len, 1u)] = w;
-  return cw;
-}
-
-// settle() for up to kBatch dependants of one lane at once: the maxima are
-// issued together, one fence orders them before the decrements, the decrements
-// are issued together, and one more fence precedes the reads of best by the
-// lanes whose decrement reached 0 -- two round trips per batch instead of two
-// per dependant.
+// Up to kBatch dependants w of one lane's vertex of color cv at once: best[w]
+// rises to cv for each (the maxima issued together), one fence orders them before
+// the decrements of pending[w] (issued together), and one more fence precedes the
+// reads of best by the lanes whose decrement reached 0, which color w with
+// best + 1 -- two round trips per batch instead of two per dependant.
 constexpr int kBatch = 4;
 __device__ __forceinline__ int32_t settle_batch(const ColorArgs& a, const int32_t (&w)[kBatch],
                                                 const int32_t (&cv)[kBatch], const bool (&ok)[kBatch], int32_t* out,
@@ -411,11 +396,8 @@ __device__ bool grid_barrier(uint32_t* bar, uint32_t& epoch, uint32_t ctas, uint
       }
       __nanosleep(32);
     }
-    if (ok) {  // acquire: every arrival's writes before what follows
-      uint32_t v;
-      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
-      (void)v;
-    }
+    if (ok)  // acquire: every arrival's writes before what follows
+      asm volatile("{\n\t.reg .u32 t;\n\tld.acquire.gpu.global.u32 t, [%0];\n\t}" ::"l"(bar) : "memory");
     s_ok = ok;
   }
   __syncthreads();

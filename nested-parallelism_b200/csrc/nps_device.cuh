@@ -1570,8 +1570,6 @@ __device__ void solve_instance(const LaunchParams& P, const InstDesc& I, Smem<BS
                                uint32_t& bar_epoch, uint32_t rank, uint32_t team_size, bool& inject) {
   constexpr int NW = BS / 32;
   Counters* ctr = I.ctr;
-  const uint32_t gthreads = team_size * BS;
-  const uint32_t gtid = rank * BS + threadIdx.x;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t gwarp = rank * NW + warp;
   const bool learned = I.policy == NPS_POLICY_LEARNED && P.policy != nullptr;
